@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Throughput of the vortexlab D2Q9 time step on B200: MLUPS and fraction of the HBM roofline.
+
+Workload (one step = one time step of the whole box, FP64 populations): the periodic 8192 x 4096
+box with seeded solid disks filling 5 % of the cells (radii 4-16, seed 0x5EED0001), BGK
+tau = 0.55, uniform start (rho, ux, uy) = (1, 0.05, 0); the force on the disks is summed every
+step. 4.8 GB of populations per buffer pair, far larger than the 126 MB L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl vortexlab|reference]
+
+Prints one JSON line. Under torchrun (N > 1) every rank runs its own replica of the box (the step
+has no data exchange between replicas); the time is the max over ranks and `value` the job total.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BOX = dict(nx=8192, ny=4096, seed=0x5EED0001, fraction=0.05, tau=0.55, u=0.05)
+BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36}
+FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes per fluid-node update of the bulk kernel from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch divided by the interior nodes it updates), per precision.
+NCU_DRAM_BYTES_PER_LU = {}
+
+
+def workload_name(prec):
+    return (f"periodic box {BOX['nx']}x{BOX['ny']}, seeded disks {int(BOX['fraction'] * 100)}% solid "
+            f"(r 4-16, seed 0x{BOX['seed']:X}), BGK tau={BOX['tau']}, u={BOX['u']}, {prec} populations")
+
+
+def hbm_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        rows = []
+        for line in open(self.path):
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 8:
+                continue
+            try:
+                rows.append((float(p[0]), float(p[1]), p[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower() == "active"})
+        loaded = [r[0] for r in rows if r[0] > 0.5 * r[1]] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows)}
+
+
+def dist_setup(world):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+    dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=300))
+    return dist
+
+
+def dist_max(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(dist, v):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def oracle_box(threads):
+    import numpy as np
+
+    import oracle as O
+    from vortexlab_b200.workloads import disk_field
+    nx, ny = BOX["nx"], BOX["ny"]
+    disks = disk_field(nx, ny, BOX["seed"], BOX["fraction"])
+    b = O.Builder(nx, ny)
+    b.periodic_x = b.periodic_y = True
+    b.tau = BOX["tau"]
+    b.collision = O.BGK
+    k = b.add_wall(fgroup=0, shape=O.Shape.disks(disks))
+    b.fill_shape(k)
+    sim = b.build(threads)
+    sim.init((np.ones((ny, nx)), np.full((ny, nx), BOX["u"]), np.zeros((ny, nx))))
+    return sim
+
+
+def time_oracle(threads, max_steps, budget_s):
+    """Times the oracle (the reference's CPU algorithm restated, row-split threads as in its pool)
+    on the box: one untimed step, then as many full steps as fit the budget (at most max_steps)."""
+    sim = oracle_box(threads)
+    t0 = time.perf_counter()
+    sim.step(1)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(max_steps, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    secs = time.perf_counter() - t0
+    return sim.fluid_nodes() * steps / secs / 1e6, steps, secs
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    mlups, steps, secs = time_oracle(threads, max(args.steps, 1), budget_s=60.0)
+    sample = f"{steps} full steps of the {BOX['nx']}x{BOX['ny']} box after 1 untimed step ({secs:.1f} s)"
+    line = {
+        "impl": "reference", "metric": "MLUPS", "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * secs / steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_name("f64"), "threads": threads},
+        "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def channel_n80(V):
+    """The reference's own benchmark (`vortexlab bench --n 80 --steps 1000`): MLUPS and state hash."""
+    ch, secs = V.cylinder.bench(V.cylinder.Setup(n=80), 1000)
+    h = ch.sim.state_hash()
+    out = {"grid": f"{ch.sim.nx}x{ch.sim.ny}", "fluid_nodes": ch.sim.fluid_nodes(), "steps": 1000,
+           "mlups": round(ch.sim.fluid_nodes() * 1000 / secs / 1e6, 1), "ms_per_step": round(secs, 6),
+           "state_hash": f"{h:016x}", "published_hash_match": f"{h:016x}" == "c93e26bfa33474ee"}
+    ch.close()
+    return out
+
+
+def run_vortexlab(args):
+    import numpy as np
+
+    import vortexlab_b200 as V
+    from vortexlab_b200.workloads import build_disk_box, disk_field
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = dist_setup(world)
+    V.set_device(local)
+    prec = args.precision
+    nx, ny = BOX["nx"], BOX["ny"]
+    t0 = time.perf_counter()
+    disks = disk_field(nx, ny, BOX["seed"], BOX["fraction"])
+    sim = build_disk_box(V, nx, ny, disks, tau=BOX["tau"], precision=prec)
+    setup_s = time.perf_counter() - t0
+    flags = sim.flags()
+    interior = int(np.count_nonzero(flags == 0))
+    fluid = sim.fluid_nodes()
+    sim.init((1.0, BOX["u"], 0.0))
+    sim.step(max(args.warmup, 3))
+    sim.synchronize()
+    if dist:
+        dist.barrier()
+    sim.synchronize()
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    gpu_index = vis.split(",")[local] if vis and len(vis.split(",")) > local else local
+    sampler = ClockSampler(gpu_index)
+    launches0 = sim.launch_count()
+    link_ms, bulk_ms, total_ms = sim.step_profiled(args.steps)
+    launches = sim.launch_count() - launches0
+    clocks = sampler.stop()
+    sim.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms_max = dist_max(dist, total_ms)
+    secs = total_ms_max * 1e-3
+    value = world * fluid * args.steps / secs / 1e6
+
+    # roofline of the dominant kernel (the bulk kernel: interior nodes, pull + collide)
+    peak, peak_kind = hbm_peak()
+    bpl = BYTES_PER_LU[prec]
+    bulk_launch_s = bulk_ms * 1e-3 / args.steps
+    achieved = interior * bpl / bulk_launch_s / 1e9
+    traffic = NCU_DRAM_BYTES_PER_LU.get(prec)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                "traffic": None if traffic is None else round(traffic * interior),
+                "kernel": "k_bulk", "algorithmic_bytes_per_launch": interior * bpl,
+                "kernel_ms_per_launch": round(bulk_ms / args.steps, 4),
+                "link_kernel_ms_per_launch": round(link_ms / args.steps, 4),
+                "bulk_share": round(bulk_ms / max(bulk_ms + link_ms, 1e-12), 4),
+                "step_frac_of_peak": round(fluid * bpl / (total_ms * 1e-3 / args.steps) / 1e9 / peak, 4)}
+
+    # end to end through the public API with host buffers: upload the start field from pinned host
+    # memory, run the steps with the per-step force recorded on the device, download the force
+    # history and the final populations.
+    n = nx * ny
+    rho_h, ux_h, uy_h, pops_h = (V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(9 * n))
+    rho_h.array[:] = 1.0
+    ux_h.array[:] = BOX["u"]
+    uy_h.array[:] = 0.0
+    sim.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    sim.init((rho_h.array.reshape(ny, nx), ux_h.array.reshape(ny, nx), uy_h.array.reshape(ny, nx)))
+    sim.record(args.steps)
+    sim.step(args.steps)
+    hist = sim.history()
+    sim.populations(out=pops_h.array)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = dist_max(dist, e2e_s)
+    e2e_value = world * fluid * args.steps / e2e_s / 1e6
+    h2d = 3 * n * 8
+    d2h = hist.nbytes + 9 * n * 8
+    finite = bool(np.isfinite(hist[:, :2]).all())
+
+    line = {
+        "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(total_ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic",
+        "config": {"workload": workload_name(prec), "grid": [nx, ny], "fluid_nodes": fluid, "interior_nodes": interior,
+                   "links": sim.link_count(), "boundary_nodes": sim.bnode_count(), "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (populations 2 x 9 x 33.5M values), no flush needed",
+                   "timing": "CUDA events around every kernel on the sim's stream, max over ranks",
+                   "setup_s": round(setup_s, 2)},
+        "roofline": roofline,
+        "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
+                "d2h_bytes_per_step": round(d2h / args.steps), "seconds": round(e2e_s, 4),
+                "path": "Sim.init(host field) + Sim.record + Sim.step + Sim.history + Sim.populations",
+                "force_finite": finite},
+        "gpu_launches": int(dist_sum(dist, launches)),
+        "clocks": clocks,
+    }
+    del rho_h, ux_h, uy_h, pops_h
+    sim.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        line["channel_n80"] = channel_n80(V)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        mlups, steps, secs = time_oracle(threads, 50, budget_s=15.0)
+        line["cpu_baseline"] = {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
+                                "sample": f"{steps} full steps of the same box after 1 untimed step ({secs:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["vortexlab", "reference"], default="vortexlab")
+    ap.add_argument("--precision", choices=["f64", "f32", "f16s"], default="f64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_vortexlab(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

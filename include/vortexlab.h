@@ -1,0 +1,236 @@
+/*
+ * vortexlab-b200 — C ABI of the B200-native D2Q9 lattice-Boltzmann time step.
+ *
+ * The reference (vortexlab, Rust) has no FFI: its boundary is the Rust `Builder` / `Sim` /
+ * `Channel` API that its cases and tests call. Every entry point below replaces one item of that
+ * API; the comment gives the reference item it replaces (file:line in the reference project).
+ *
+ * Conventions
+ *  - Plain C types only: pointers, sizes, doubles. Host arrays are row-major with x fastest
+ *    (cell index idx = y * nx + x), as in the reference (src/sim.rs:251).
+ *  - Population arrays exchanged with the host use the reference layout: population i of cell idx
+ *    at i * n + idx, n = nx * ny (src/sim.rs:335-336). The device layout pads each population
+ *    plane to a 64-element boundary; that padding never crosses this ABI.
+ *  - Every function that can fail returns an int status: VL_OK (0) or a negative VL_E* code,
+ *    with a message from vl_last_error() (thread-local). Where the reference panics on a contract
+ *    violation (src/sim.rs:85, :101, :222, :261, :303) this ABI returns VL_EINVAL instead; it
+ *    never aborts the process. Constructors return NULL on failure.
+ *  - One vl_sim is driven from one host thread; it owns one CUDA stream on the device that was
+ *    current when it was built. There is no CPU fallback: without a CUDA device every vl_sim
+ *    constructor fails with VL_ECUDA.
+ */
+#ifndef VORTEXLAB_H
+#define VORTEXLAB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VL_ABI_VERSION 1
+
+/* ---- status codes */
+#define VL_OK 0
+#define VL_EINVAL (-1)       /* contract violation (the reference panics)                      */
+#define VL_ECUDA (-2)        /* CUDA runtime error or no CUDA device                           */
+#define VL_EDIVERGED (-3)    /* non-finite force: src/cases/cylinder.rs:397-404, tunnel.rs:78-84 */
+#define VL_ENOMEM (-4)       /* device or host allocation failed                               */
+#define VL_EUNSUPPORTED (-5) /* valid request that this build does not implement               */
+
+/* ---- enums */
+enum { VL_BGK = 0, VL_TRT = 1 };                              /* src/lattice.rs:28-35 */
+enum { VL_F64 = 0, VL_F32 = 1, VL_F16S = 2 };                 /* population storage    */
+enum { VL_VEL_NONE = 0, VL_VEL_CONST = 1, VL_VEL_PARABOLIC = 2, VL_VEL_ROTATION = 3 };
+enum { VL_CORNER_SHARP = 0, VL_CORNER_CHAMFERED = 1, VL_CORNER_ROUNDED = 2,
+       VL_CORNER_RECESSED = 3, VL_CORNER_DOUBLE_RECESSED = 4 }; /* src/geometry.rs:188-201 */
+enum { VL_INFLOW_PARABOLIC = 0, VL_INFLOW_UNIFORM = 1, VL_INFLOW_UNIFORM_OPEN = 2 }; /* channel.rs:22-33 */
+
+#define VL_VGROUPS 4   /* src/sim.rs:67 */
+#define VL_MAX_FGROUPS 4  /* force groups per sim (the reference has no limit; see vl_builder_add_wall) */
+
+typedef struct vl_shape vl_shape;
+typedef struct vl_builder vl_builder;
+typedef struct vl_sim vl_sim;
+typedef struct vl_channel vl_channel;
+
+/* Wall velocity as tagged data; replaces the closure `VelocityFn` (src/sim.rs:34), which C
+ * cannot carry. The forms are exactly the closures the reference's cases build:
+ *   VL_VEL_CONST      p = {ux, uy}              -> [ux, uy]
+ *   VL_VEL_PARABOLIC  p = {u_mean, h}           -> [6 u_mean s (h - s) / h^2, 0], s = clamp(y - 1/2, 0, h)
+ *                                                  (src/cases/channel.rs:77-86)
+ *   VL_VEL_ROTATION   p = {cx, cy}              -> [-(y - cy), x - cx] (src/cases/channel.rs:104) */
+typedef struct {
+  int kind;
+  double p[4];
+} vl_velocity;
+
+/* src/sim.rs:38-49 (`Wall`). fgroup < 0 means no force bookkeeping. `shape` (may be NULL) is
+ * owned by the builder after vl_builder_add_wall returns, whether or not the call succeeds. */
+typedef struct {
+  vl_velocity velocity;
+  int vgroup;
+  int fgroup;
+  vl_shape* shape;
+} vl_wall;
+
+const char* vl_last_error(void);
+/* Status code of the last failure on this thread (for constructors, which return NULL). */
+int vl_last_status(void);
+int vl_abi_version(void);
+/* Number of CUDA devices visible (0 on a machine without GPU). */
+int vl_device_count(void);
+/* Makes `device` current for this host thread; sims built afterwards live on it. */
+int vl_set_device(int device);
+/* Page-locked host buffers (for fast, asynchronous host<->device copies); NULL on failure. */
+void* vl_pinned_alloc(size_t bytes);
+void vl_pinned_free(void* p);
+
+/* ================================================================ shapes: src/geometry.rs */
+vl_shape* vl_shape_circle(double cx, double cy, double r);                 /* :16-27  */
+vl_shape* vl_shape_polygon(const double* xy, size_t npts);                 /* :30-49, xy = x0,y0,x1,y1,... */
+vl_shape* vl_shape_rounded_square(double cx, double cy, double half, double r); /* :52-66 */
+vl_shape* vl_shape_rotated(vl_shape* inner, double cx, double cy, double angle); /* :69-82, takes inner */
+vl_shape* vl_shape_translated(vl_shape* inner, double dx, double dy);      /* :85-95, takes inner */
+vl_shape* vl_shape_section(int corner, double b, double cx, double cy, double d, double angle); /* :251-261 */
+vl_shape* vl_shape_bitmap(size_t w, size_t h, const float* level, double x0, double y0, double scale); /* :120-185 */
+vl_shape* vl_shape_outside_band(double y0, double y1);                     /* src/cases/poiseuille.rs:12-21 */
+/* New body classes for the batched tunnels (no reference counterpart). */
+vl_shape* vl_shape_ellipse(double cx, double cy, double a, double b);
+vl_shape* vl_shape_star(double cx, double cy, const double* radii, size_t nvert, double phase);
+/* Union of disks given as (cx, cy, r) triples: inside if any disk contains the point (the disk
+ * test of Circle, src/geometry.rs:22-27). Used for the seeded obstacle field of the periodic box. */
+vl_shape* vl_shape_disks(const double* cxcyr, size_t ndisks);
+void vl_shape_free(vl_shape* s);
+int vl_shape_inside(const vl_shape* s, double x, double y);                /* Shape::inside :12-14 */
+double vl_cut_fraction(const vl_shape* s, double x, double y, double dx, double dy); /* :268-279 */
+/* out = {x_min, x_max, y_min, y_max}; returns 1 if found, 0 if nothing inside (:99-115). */
+int vl_bounding_box(const vl_shape* s, double reach, double step, double* out);
+
+/* ================================================================ builder: src/sim.rs:70-137 */
+vl_builder* vl_builder_new(size_t nx, size_t ny);                          /* Builder::new :84-97 */
+void vl_builder_free(vl_builder* b);
+int vl_builder_set_periodic(vl_builder* b, int periodic_x, int periodic_y); /* pub fields :73-74 */
+int vl_builder_set_tau(vl_builder* b, double tau);                         /* :75 */
+int vl_builder_set_collision(vl_builder* b, int collision, double magic);  /* :76 */
+int vl_builder_set_accel(vl_builder* b, double gx, double gy);             /* :78 */
+/* Builder::add(Kind::Wall) :100-104. Returns the kind id (1..254) or a negative status. */
+int vl_builder_add_wall(vl_builder* b, const vl_wall* wall);
+int vl_builder_add_static_wall(vl_builder* b);                             /* :107-109 */
+int vl_builder_add_pressure(vl_builder* b, double rho);                    /* Kind::Pressure :56 */
+int vl_builder_add_radiating(vl_builder* b, double rho);                   /* Kind::Radiating :62 */
+int vl_builder_fill_rect(vl_builder* b, size_t x0, size_t x1, size_t y0, size_t y1, int kind); /* :112-118 */
+int vl_builder_fill_shape(vl_builder* b, int kind);                        /* :121-132 */
+/* Host-side view of the link tables Sim::from_builder would build (src/sim.rs:243-328), without
+ * touching a GPU. Call with NULL arrays to get the counts, then with arrays of n (flags), nbnodes
+ * (bnode_idx), nbnodes + 1 (bnode_first), 5 * nlinks (link_f64 = q, cu6, uw_x, uw_y, rho) and
+ * 7 * nlinks (link_i32 = dir, pressure, radiating, vgroup, fgroup, behind, normal code
+ * 1 + (nx + 1) + 3 * ny) values. For testing the host compiler against the oracle. */
+int vl_builder_link_table(vl_builder* b, size_t* nlinks, size_t* nbnodes, size_t* npnodes, uint8_t* flags,
+                          int32_t* bnode_idx, int32_t* bnode_first, double* link_f64, int32_t* link_i32);
+/* Builder::build + Sim::from_builder (:134-136, :219-354): classifies the cells, builds the
+ * boundary-node and link lists once on the host, uploads them and allocates the population
+ * buffers in the given storage precision. Consumes `b` (freed on success and on failure). */
+vl_sim* vl_builder_build(vl_builder* b, int precision);
+
+/* ================================================================ sim: src/sim.rs:180-673 */
+void vl_sim_free(vl_sim* s);
+int vl_sim_info(const vl_sim* s, size_t* nx, size_t* ny, size_t* fluid_nodes, size_t* link_count,
+                size_t* bnode_count, int* ngroups, int* precision);        /* fluid_nodes :377, link_count :386 */
+/* Sim::init :357-371 with the field given as three host arrays of n values (x fastest).
+ * NULL arrays mean the uniform values (rho0, ux0, uy0). Solid cells get (1, 0, 0). Resets t. */
+int vl_sim_init(vl_sim* s, const double* rho, const double* ux, const double* uy,
+                double rho0, double ux0, double uy0);
+/* Sim::step :391-420, `steps` times, queued on the sim's stream (returns before completion). */
+int vl_sim_step(vl_sim* s, uint64_t steps);
+int vl_sim_synchronize(vl_sim* s);
+int vl_sim_set_vscale(vl_sim* s, int group, double value);                 /* pub vscale :196 */
+int vl_sim_get_vscale(const vl_sim* s, double* out4);
+int vl_sim_set_outflow_target(vl_sim* s, int enabled, double target);      /* pub outflow_target :208 */
+int vl_sim_outlet_density_offset(vl_sim* s, double* out);                 /* pub outlet_density_offset :210 */
+int vl_sim_t(vl_sim* s, uint64_t* t);                                      /* pub t :214 */
+/* Divergence check: nonfinite = 1 once a step produced a non-finite force, with the step index
+ * (t before that step). The reference's cases test `!cd.is_finite()` after every step
+ * (src/cases/cylinder.rs:397-404, src/cases/tunnel.rs:78-84); here the device records it. */
+int vl_sim_status(vl_sim* s, int* nonfinite, uint64_t* first_t);
+/* pub force :198 — force[g] = (fx, fy) of the last step; out holds 2 * ngroups doubles. */
+int vl_sim_force(vl_sim* s, double* out);
+/* All populations (FP64, reference layout, 9 * n values) of the current state (`a`). */
+int vl_sim_download(vl_sim* s, double* out);
+/* Replaces the current populations (FP64, reference layout). */
+int vl_sim_upload(vl_sim* s, const double* in);
+int vl_sim_flags(vl_sim* s, uint8_t* out);                                 /* flag :187-188: 0 interior, 1 boundary, 2 solid */
+int vl_sim_macros_field(vl_sim* s, double* rho, double* ux, double* uy);   /* Sim::macros :527-534 over all cells */
+int vl_sim_macros(vl_sim* s, size_t x, size_t y, double* out3);            /* Sim::macros :527-534 */
+int vl_sim_total_mass(vl_sim* s, double* out);                             /* :538-548, on the device in FP64 */
+int vl_sim_total_momentum(vl_sim* s, double* out2);                        /* :551-563, on the device in FP64 */
+int vl_sim_max_speed(vl_sim* s, double* out);                              /* :566-579 (NaN on blow-up) */
+int vl_sim_vorticity(vl_sim* s, float* out);                               /* :582-620 */
+int vl_sim_probe_density(vl_sim* s, double x, double y, double* out);      /* :624-644 */
+int vl_sim_probe_density_at_wall(vl_sim* s, double x, double y, double nx, double ny, double* out); /* :648-651 */
+int vl_sim_state_hash(vl_sim* s, uint64_t* out);                           /* :654-668 */
+
+/* ---- per-step recording (the device writes, the host downloads in bulk)
+ * While enabled, every step appends one record of VL_REC doubles to a device history:
+ *   [0 .. 2*VL_MAX_FGROUPS)  force[g] = (fx, fy) for g < ngroups (zeros above)
+ *   [8]  outlet density offset used in that step
+ *   [9]  pressure-drop probe value after that step (see vl_sim_set_dp_probe), else 0
+ * Replaces the per-step host reads of Channel::coefficients (src/cases/channel.rs:133-136) and
+ * Rig::pressure_drop (src/cases/cylinder.rs:272-277). */
+#define VL_REC 10
+int vl_sim_record(vl_sim* s, uint64_t capacity);   /* 0 disables; (re)starts at the next step */
+int vl_sim_history(vl_sim* s, double* out, uint64_t* count);  /* out: count * VL_REC doubles */
+/* Pressure drop CS2 (p_front - p_back) / u_ref^2 between the wall points (xc - r, yc) and
+ * (xc + r, yc), each from Sim::probe_density_at_wall, evaluated on the device after every step. */
+int vl_sim_set_dp_probe(vl_sim* s, double xc, double yc, double r, double u_ref);
+/* Device time of the last vl_sim_step batch in milliseconds (CUDA events on the sim's stream). */
+int vl_sim_last_step_ms(vl_sim* s, float* ms);
+/* Runs `steps` steps launched one at a time with CUDA events around every kernel on the sim's
+ * stream; returns the summed device milliseconds of the link kernels, of the bulk kernels and of
+ * the whole batch (any pointer may be NULL). Used to measure each kernel's share of a step. */
+int vl_sim_step_profiled(vl_sim* s, uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms);
+/* Number of kernel launches issued by this sim so far (steps launch one or two kernels each). */
+int vl_sim_launch_count(vl_sim* s, uint64_t* out);
+
+/* ================================================================ channel: src/cases/channel.rs */
+/* Spec :47-58 plus Kick :37-45. `body` is owned by the channel after the call. */
+typedef struct {
+  size_t nx, ny;
+  int inflow;       /* VL_INFLOW_* */
+  double u;         /* u_mean (parabolic) or u (uniform) */
+  double nu;
+  int collision;
+  double magic;
+  vl_shape* body;
+  uint64_t ramp_steps;
+  int has_kick;
+  double kick_cx, kick_cy, kick_omega;
+  uint64_t kick_start, kick_duration;
+} vl_channel_spec;
+
+vl_channel* vl_channel_new(const vl_channel_spec* spec, int precision);  /* Channel::new :71-116 */
+void vl_channel_free(vl_channel* c);
+vl_sim* vl_channel_sim(vl_channel* c);                                     /* pub sim :61 */
+int vl_channel_set_absorbing(vl_channel* c, int on);                       /* pub absorbing_outlet :67 */
+/* Channel::step :118-130, `steps` times. The per-step controls (inlet ramp, outlet target, body
+ * kick) come from a schedule uploaded once, so a batch of steps needs no host round trip. */
+int vl_channel_step(vl_channel* c, uint64_t steps);
+int vl_channel_coefficients(vl_channel* c, double d, double* cd, double* cl); /* :133-136 */
+double vl_channel_u_ref(const vl_channel* c);
+
+/* ================================================================ signal: src/signal.rs */
+int vl_fft(double* re, double* im, size_t n);                              /* :6-44 */
+double vl_mean(const double* x, size_t n);                                 /* :61-63 */
+double vl_rms(const double* x, size_t n);                                  /* :66-69 */
+int vl_dominant_frequency(const double* x, size_t n, double dt, double* freq, double* amp); /* :92-107 */
+size_t vl_peaks(const double* x, size_t n, double* pos, double* val, size_t cap);           /* :111-123 */
+int vl_crossing_frequency(const double* x, size_t n, double dt, double* out);                /* :127-140 */
+double vl_sample_at(const double* x, size_t n, double pos);                /* :143-147 */
+double vl_ramp(uint64_t t, uint64_t steps);                                /* src/cases/mod.rs:11-18 */
+double vl_tau_for(double nu);                                              /* src/lattice.rs:53-55 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VORTEXLAB_H */

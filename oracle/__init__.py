@@ -61,6 +61,7 @@ def _declare(L):
         "vlo_shape_ellipse": (vp, [d, d, d, d]),
         "vlo_shape_section": (vp, [i, d, d, d, d, d]),
         "vlo_shape_bitmap": (vp, [sz, sz, P(C.c_float), d, d, d]),
+        "vlo_shape_disks": (vp, [P(d), sz]),
         "vlo_shape_free": (None, [vp]),
         "vlo_shape_inside": (i, [vp, d, d]),
         "vlo_cut_fraction": (d, [vp, d, d, d, d]),
@@ -86,6 +87,7 @@ def _declare(L):
         "vlo_sim_t": (u64, [vp]),
         "vlo_sim_flags": (None, [vp, P(C.c_uint8)]),
         "vlo_sim_init_arrays": (None, [vp, P(d), P(d), P(d)]),
+        "vlo_sim_link_table": (None, [vp, P(C.c_int32), P(C.c_int32), P(d), P(C.c_int32)]),
         "vlo_sim_step": (None, [vp, u64]),
         "vlo_sim_set_vscale": (None, [vp, i, d]),
         "vlo_sim_get_vscale": (d, [vp, i]),
@@ -243,6 +245,11 @@ class Shape:
     @staticmethod
     def ellipse(cx, cy, a, b):
         return Shape(lib().vlo_shape_ellipse(cx, cy, a, b))
+
+    @staticmethod
+    def disks(cxcyr):
+        a = _arr(cxcyr).reshape(-1)
+        return Shape(lib().vlo_shape_disks(_dp(a), len(a) // 3))
 
     @staticmethod
     def section(corner, b, cx, cy, d, angle=0.0):
@@ -446,6 +453,18 @@ class Sim:
 
     def state_hash(self):
         return lib().vlo_sim_state_hash(self.ptr)
+
+    def link_table(self):
+        nb, nl = self.bnode_count(), self.link_count()
+        bidx = np.zeros(nb, dtype=np.int32)
+        bfirst = np.zeros(nb + 1, dtype=np.int32)
+        lf = np.zeros(5 * max(nl, 1))
+        li = np.zeros(7 * max(nl, 1), dtype=np.int32)
+        P32 = C.POINTER(C.c_int32)
+        lib().vlo_sim_link_table(self.ptr, bidx.ctypes.data_as(P32), bfirst.ctypes.data_as(P32), _dp(lf),
+                                 li.ctypes.data_as(P32))
+        return dict(flags=self.flags(), bnode_idx=bidx, bnode_first=bfirst, link_f64=lf[:5 * nl].reshape(-1, 5),
+                    link_i32=li[:7 * nl].reshape(-1, 7), npnodes=self.pnode_count())
 
 
 # ------------------------------------------------------------------ cases

@@ -225,6 +225,35 @@ struct Ellipse : Shape {
   }
 };
 
+// Union of disks: inside if any Circle (src/geometry.rs:22-27) contains the point. Plain scan over
+// the disks whose bounding box contains the point (a sorted sweep on x keeps it fast).
+struct DiskUnion : Shape {
+  std::vector<double> cx, cy, r;
+  std::vector<size_t> order;  // by cx - r
+  double rmax = 0.0;
+  void prepare() {
+    order.resize(cx.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cx[a] - r[a] < cx[b] - r[b]; });
+    for (double v : r) rmax = std::max(rmax, v);
+  }
+  bool inside(double x, double y) const override {
+    // first disk whose left edge could be at or left of x
+    size_t lo = 0, hi = order.size();
+    while (lo < hi) {
+      size_t mid = (lo + hi) / 2;
+      if (cx[order[mid]] - r[order[mid]] <= x) lo = mid + 1; else hi = mid;
+    }
+    for (size_t m = lo; m-- > 0;) {
+      size_t k = order[m];
+      if (cx[k] + rmax < x - rmax) break;
+      double dx = x - cx[k], dy = y - cy[k];
+      if (dx * dx + dy * dy < r[k] * r[k]) return true;
+    }
+    return false;
+  }
+};
+
 // src/geometry.rs:120-185
 struct Bitmap : Shape {
   size_t w = 0, h = 0;
@@ -1139,6 +1168,12 @@ void* vlo_shape_bitmap(size_t w, size_t h, const float* level, double x0, double
   auto s = new Bitmap(); s->w = w; s->h = h; s->level.assign(level, level + w * h);
   s->x0 = x0; s->y0 = y0; s->scale = scale; return (Shape*)s;
 }
+void* vlo_shape_disks(const double* cxcyr, size_t n) {
+  auto s = new DiskUnion();
+  for (size_t k = 0; k < n; ++k) { s->cx.push_back(cxcyr[3 * k]); s->cy.push_back(cxcyr[3 * k + 1]); s->r.push_back(cxcyr[3 * k + 2]); }
+  s->prepare();
+  return (Shape*)s;
+}
 void vlo_shape_free(void* s) { delete (Shape*)s; }
 int vlo_shape_inside(void* s, double x, double y) { return ((Shape*)s)->inside(x, y) ? 1 : 0; }
 double vlo_cut_fraction(void* s, double x, double y, double dx, double dy) {
@@ -1219,6 +1254,28 @@ void vlo_sim_flags(void* s, uint8_t* out) {
   auto p = (Sim*)s; std::memcpy(out, p->flag.data(), p->n);
 }
 // Field init from arrays of n = nx*ny values (x fastest).
+// Link list of Sim::from_builder in the same encoding as the product's vl_builder_link_table.
+void vlo_sim_link_table(void* sp, int32_t* bnode_idx, int32_t* bnode_first, double* link_f64, int32_t* link_i32) {
+  auto s = (Sim*)sp;
+  for (size_t k = 0; k < s->bnodes.size(); ++k) {
+    if (bnode_idx) bnode_idx[k] = (int32_t)s->bnodes[k].idx;
+    if (bnode_first) { bnode_first[k] = (int32_t)s->bnodes[k].first; bnode_first[k + 1] = (int32_t)s->bnodes[k].last; }
+  }
+  for (size_t k = 0; k < s->links.size(); ++k) {
+    const Link& L = s->links[k];
+    if (link_f64) {
+      double* o = link_f64 + 5 * k;
+      o[0] = L.q; o[1] = L.cu6; o[2] = L.uw[0]; o[3] = L.uw[1]; o[4] = L.rho;
+    }
+    if (link_i32) {
+      int32_t* o = link_i32 + 7 * k;
+      o[0] = L.dir; o[1] = L.kind; o[2] = L.radiating ? 1 : 0; o[3] = L.vgroup;
+      o[4] = L.fgroup == NONE ? -1 : (int32_t)L.fgroup;
+      o[5] = L.behind == NONE ? -1 : (int32_t)L.behind;
+      o[6] = L.normal[0] + 3 * (L.normal[1] + 1) + 1;
+    }
+  }
+}
 void vlo_sim_init_arrays(void* sp, const double* rho, const double* ux, const double* uy) {
   auto s = (Sim*)sp;
   s->init_fn([&](size_t x, size_t y, double* r) {

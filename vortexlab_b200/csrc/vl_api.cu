@@ -1,0 +1,1202 @@
+// C ABI of vortexlab-b200 (include/vortexlab.h): shapes, builder, device-resident sims, the
+// channel case and signal analysis. Host code; the kernels live in vl_step_*.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/vortexlab.h"
+#include "vl_device.cuh"
+#include "vl_host.hpp"
+#include "vl_launch.hpp"
+
+struct vl_shape {
+  std::unique_ptr<vl::Shape> s;
+};
+struct vl_builder {
+  vl::DomainSpec spec;
+};
+
+namespace {
+
+thread_local std::string g_err;
+thread_local int g_code = VL_OK;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  g_code = code;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? VL_ENOMEM : VL_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VL_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+vl_shape* wrap_shape(std::unique_ptr<vl::Shape> s) {
+  auto w = new vl_shape();
+  w->s = std::move(s);
+  return w;
+}
+
+constexpr int kGraphSteps = 32;  // steps per captured CUDA graph (even: buffer parity returns)
+constexpr int kReduceBlocks = 296;
+
+}  // namespace
+
+// ==================================================================== device-resident sim
+struct vl_sim {
+  int device = 0;
+  int prec = VL_F64;
+  const vl::Launchers* L = nullptr;
+  vl::CompiledDomain dom;
+  size_t n = 0;
+  unsigned ns = 0;
+  void* buf[2] = {nullptr, nullptr};
+  int cur = 0;
+  uint8_t* d_flag = nullptr;
+  int32_t* d_bidx = nullptr;
+  int32_t* d_bfirst = nullptr;
+  vl::LinkRecDev* d_links = nullptr;
+  int32_t* d_pidx = nullptr;
+  int8_t* d_pn = nullptr;
+  vl::Ctl* d_ctl = nullptr;
+  double* d_partials = nullptr;
+  double* d_hist = nullptr;
+  double* d_sched = nullptr;
+  double* d_red = nullptr;
+  int32_t* d_cells = nullptr;
+  double* d_gather = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  vl::StepParams P{};
+  int ck = 1;
+  cudaGraphExec_t gexec = nullptr;
+  uint64_t launches = 0;
+  int kernels_per_step = 1;
+  uint64_t t_host = 0;
+  uint64_t rec_start = 0, rec_cap = 0;
+  bool timed = false;
+  // host mirror of the control block
+  vl::Ctl hctl{};
+
+  ~vl_sim() {
+    if (device >= 0) cudaSetDevice(device);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_ctl,
+                    d_partials, d_hist, d_sched, d_red, d_cells, d_gather};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+    for (cudaEvent_t e : pev) cudaEventDestroy(e);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  const void* a() const { return buf[cur]; }
+  void* b() const { return buf[cur ^ 1]; }
+
+  int push_ctl() {
+    VL_CUDA(cudaMemcpyAsync(d_ctl, &hctl, sizeof(vl::Ctl), cudaMemcpyHostToDevice, stream));
+    return VL_OK;
+  }
+  // Reads the device control block into the host mirror (synchronises the stream).
+  int pull_ctl() {
+    VL_CUDA(cudaMemcpyAsync(&hctl, d_ctl, sizeof(vl::Ctl), cudaMemcpyDeviceToHost, stream));
+    VL_CUDA(cudaStreamSynchronize(stream));
+    return VL_OK;
+  }
+
+  int launch_one() {
+    cudaError_t e = L->step(P, ck, a(), b(), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "step launch");
+    cur ^= 1;
+    launches += (uint64_t)kernels_per_step;
+    return VL_OK;
+  }
+
+  int ensure_graph() {
+    if (gexec) return VL_OK;
+    cudaGraph_t g = nullptr;
+    VL_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int saved = cur;
+    cur = 0;
+    for (int k = 0; k < kGraphSteps; ++k) {
+      cudaError_t e = L->step(P, ck, a(), b(), stream);
+      cur ^= 1;
+      if (e != cudaSuccess) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        cur = saved;
+        return cuda_fail(e, "graph capture");
+      }
+    }
+    cur = saved;
+    VL_CUDA(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "graph instantiate");
+    return VL_OK;
+  }
+
+  int step(uint64_t steps) {
+    VL_CUDA(cudaSetDevice(device));
+    VL_CUDA(cudaEventRecord(ev0, stream));
+    uint64_t left = steps;
+    while (left > 0) {
+      if (left >= (uint64_t)kGraphSteps && cur == 0) {
+        int rc = ensure_graph();
+        if (rc) return rc;
+        VL_CUDA(cudaGraphLaunch(gexec, stream));
+        launches += (uint64_t)kGraphSteps * kernels_per_step;
+        left -= kGraphSteps;
+      } else {
+        int rc = launch_one();
+        if (rc) return rc;
+        left -= 1;
+      }
+    }
+    VL_CUDA(cudaEventRecord(ev1, stream));
+    timed = true;
+    t_host += steps;
+    return VL_OK;
+  }
+
+  // Steps launched one by one with CUDA events around each kernel on the sim's stream; returns
+  // the summed device time of the link kernels, of the bulk kernels and of the whole batch.
+  std::vector<cudaEvent_t> pev;
+  int step_profiled(uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms) {
+    VL_CUDA(cudaSetDevice(device));
+    const size_t need = 2 * (size_t)steps + 1;
+    while (pev.size() < need) {
+      cudaEvent_t e;
+      VL_CUDA(cudaEventCreate(&e));
+      pev.push_back(e);
+    }
+    const bool has_links = P.nlink > 0;
+    VL_CUDA(cudaEventRecord(pev[0], stream));
+    for (uint64_t k = 0; k < steps; ++k) {
+      // links then bulk, as one step launches them, with an event after each
+      cudaError_t e = cudaSuccess;
+      if (has_links) e = L->step(P, ck | 0x100, a(), b(), stream);
+      if (e != cudaSuccess) return cuda_fail(e, "profiled step");
+      VL_CUDA(cudaEventRecord(pev[2 * k + 1], stream));
+      e = L->step(P, ck | 0x200, a(), b(), stream);
+      if (e != cudaSuccess) return cuda_fail(e, "profiled step");
+      VL_CUDA(cudaEventRecord(pev[2 * k + 2], stream));
+      cur ^= 1;
+      launches += (uint64_t)kernels_per_step;
+    }
+    VL_CUDA(cudaEventSynchronize(pev[2 * steps]));
+    double lk = 0.0, bk = 0.0;
+    for (uint64_t k = 0; k < steps; ++k) {
+      float m1 = 0.f, m2 = 0.f;
+      VL_CUDA(cudaEventElapsedTime(&m1, pev[2 * k], pev[2 * k + 1]));
+      VL_CUDA(cudaEventElapsedTime(&m2, pev[2 * k + 1], pev[2 * k + 2]));
+      lk += m1;
+      bk += m2;
+    }
+    float tot = 0.f;
+    VL_CUDA(cudaEventElapsedTime(&tot, pev[0], pev[2 * steps]));
+    if (link_ms) *link_ms = lk;
+    if (bulk_ms) *bulk_ms = bk;
+    if (total_ms) *total_ms = tot;
+    t_host += steps;
+    return VL_OK;
+  }
+
+  // 9 FP64 populations of each listed cell (reference order).
+  int gather(const std::vector<int32_t>& cells, std::vector<double>& out) {
+    out.assign(cells.size() * 9, 0.0);
+    if (cells.empty()) return VL_OK;
+    if (cells.size() > 64) return fail(VL_EINVAL, "gather: too many cells");
+    VL_CUDA(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(int32_t), cudaMemcpyHostToDevice, stream));
+    cudaError_t e = L->gather((int)cells.size(), ns, d_cells, a(), d_gather, stream);
+    if (e != cudaSuccess) return cuda_fail(e, "gather");
+    VL_CUDA(cudaMemcpyAsync(out.data(), d_gather, out.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    VL_CUDA(cudaStreamSynchronize(stream));
+    return VL_OK;
+  }
+};
+
+namespace {
+
+// Bilinear probe weights of Sim::probe_density (src/sim.rs:624-644) for the point (x, y): up to
+// four (cell, weight) pairs, in the reference's corner order, for fluid cells with weight > 0.
+void probe_corners(const vl_sim& s, double x, double y, int32_t* idx, double* w) {
+  const double i = std::floor(x), j = std::floor(y);
+  const double fx = x - i, fy = y - j;
+  const long di[4] = {0, 1, 0, 1}, dj[4] = {0, 0, 1, 1};
+  const double wk[4] = {(1.0 - fx) * (1.0 - fy), fx * (1.0 - fy), (1.0 - fx) * fy, fx * fy};
+  for (int k = 0; k < 4; ++k) {
+    idx[k] = -1;
+    w[k] = 0.0;
+    const long xi = (long)i + di[k], yj = (long)j + dj[k];
+    if (xi < 0 || yj < 0 || xi >= (long)s.dom.nx || yj >= (long)s.dom.ny) continue;
+    const size_t c = (size_t)yj * s.dom.nx + (size_t)xi;
+    if (s.dom.flag[c] != 2 && wk[k] > 0.0) {
+      idx[k] = (int32_t)c;
+      w[k] = wk[k];
+    }
+  }
+}
+
+void moments_host(const double* f, double& rho, double& jx, double& jy) { vl::moments(f, rho, jx, jy); }
+
+int sim_probe_density(vl_sim* s, double x, double y, double* out) {
+  int32_t idx[4];
+  double w[4];
+  probe_corners(*s, x, y, idx, w);
+  std::vector<int32_t> cells;
+  for (int k = 0; k < 4; ++k)
+    if (idx[k] >= 0) cells.push_back(idx[k]);
+  std::vector<double> f;
+  int rc = s->gather(cells, f);
+  if (rc) return rc;
+  double sum = 0.0, wsum = 0.0;
+  size_t m = 0;
+  for (int k = 0; k < 4; ++k) {
+    if (idx[k] < 0) continue;
+    double rho, jx, jy;
+    moments_host(&f[9 * m], rho, jx, jy);
+    ++m;
+    sum += w[k] * rho;
+    wsum += w[k];
+  }
+  *out = wsum > 0.0 ? sum / wsum : std::nan("");
+  return VL_OK;
+}
+
+int alloc_copy(void** dst, const void* src, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  VL_CUDA(cudaMalloc(dst, bytes));
+  if (src) VL_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  return VL_OK;
+}
+
+// Creates the device-resident sim for a compiled domain.
+vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    fail(VL_ECUDA, "no CUDA device: vortexlab-b200 has no CPU fallback");
+    return nullptr;
+  }
+  auto s = std::make_unique<vl_sim>();
+  if (cudaGetDevice(&s->device) != cudaSuccess) {
+    fail(VL_ECUDA, "cudaGetDevice failed");
+    return nullptr;
+  }
+  s->prec = precision;
+  switch (precision) {
+    case VL_F64: s->L = &vl::launchers_f64(); break;
+    case VL_F32: s->L = &vl::launchers_f32(); break;
+    case VL_F16S: s->L = &vl::launchers_f16s(); break;
+    default: fail(VL_EINVAL, "unknown precision"); return nullptr;
+  }
+  s->dom = std::move(dom);
+  vl::CompiledDomain& d = s->dom;
+  s->n = d.n;
+  s->ns = (unsigned)((d.n + 63) / 64 * 64);
+  if ((unsigned long long)s->ns * 9ull > 0xFFFFFFFFull) {
+    fail(VL_EINVAL, "grid too large: 9 population planes must fit 32-bit offsets");
+    return nullptr;
+  }
+  auto chk = [&](int rc) { return rc == VL_OK; };
+  const size_t pop_bytes = (size_t)s->ns * 9 * s->L->elem;
+  if (!chk(alloc_copy(&s->buf[0], nullptr, pop_bytes)) || !chk(alloc_copy(&s->buf[1], nullptr, pop_bytes)))
+    return nullptr;
+  if (cudaMemset(s->buf[0], 0, pop_bytes) != cudaSuccess || cudaMemset(s->buf[1], 0, pop_bytes) != cudaSuccess) {
+    fail(VL_ECUDA, "memset");
+    return nullptr;
+  }
+  std::vector<vl::LinkRecDev> links(d.links.size());
+  for (size_t k = 0; k < d.links.size(); ++k) {
+    const vl::LinkRec& h = d.links[k];
+    vl::LinkRecDev& g = links[k];
+    g.q = h.q; g.cu6 = h.cu6; g.uw0 = h.uw[0]; g.uw1 = h.uw[1]; g.rho = h.rho;
+    g.behind = h.behind; g.dir = h.dir; g.flags = h.flags; g.vgroup = h.vgroup; g.fgroup = h.fgroup;
+  }
+  std::vector<int8_t> pn(2 * d.pnode_idx.size());
+  for (size_t k = 0; k < d.pnode_idx.size(); ++k) { pn[2 * k] = d.pnode_nx[k]; pn[2 * k + 1] = d.pnode_ny[k]; }
+  if (!chk(alloc_copy((void**)&s->d_flag, d.flag.data(), d.n)) ||
+      !chk(alloc_copy((void**)&s->d_bidx, d.bnode_idx.data(), d.bnode_idx.size() * 4)) ||
+      !chk(alloc_copy((void**)&s->d_bfirst, d.bnode_first.data(), d.bnode_first.size() * 4)) ||
+      !chk(alloc_copy((void**)&s->d_links, links.data(), links.size() * sizeof(vl::LinkRecDev))) ||
+      !chk(alloc_copy((void**)&s->d_pidx, d.pnode_idx.data(), d.pnode_idx.size() * 4)) ||
+      !chk(alloc_copy((void**)&s->d_pn, pn.data(), pn.size())) ||
+      !chk(alloc_copy((void**)&s->d_ctl, nullptr, sizeof(vl::Ctl))) ||
+      !chk(alloc_copy((void**)&s->d_red, nullptr, kReduceBlocks * 7 * sizeof(double))) ||
+      !chk(alloc_copy((void**)&s->d_cells, nullptr, 64 * sizeof(int32_t))) ||
+      !chk(alloc_copy((void**)&s->d_gather, nullptr, 64 * 9 * sizeof(double))))
+    return nullptr;
+  if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
+    fail(VL_ECUDA, "stream/event creation");
+    return nullptr;
+  }
+  // Launch geometry: the bulk kernel sized to one full wave of resident blocks (grid-stride over
+  // row tiles); the link kernel to at most two blocks per SM.
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  const bool forced = d.accel[0] != 0.0 || d.accel[1] != 0.0;
+  s->ck = forced ? 2 : (d.collision == vl::COLL_BGK ? 0 : 1);
+  vl::StepParams& P = s->P;
+  P.nx = (int)d.nx;
+  P.ny = (int)d.ny;
+  P.ns = s->ns;
+  P.tiles_per_row = (int)((d.nx + vl::kBlock - 1) / vl::kBlock);
+  P.ntiles = P.tiles_per_row * (int)d.ny;
+  const int occ = s->L->bulk_occupancy(s->ck);
+  P.nbulk = std::max(1, std::min(P.ntiles, sms * occ));
+  const int nb = (int)d.bnode_idx.size();
+  P.nlink = nb == 0 ? 0 : std::max(1, std::min((nb + vl::kBlock - 1) / vl::kBlock, 2 * sms));
+  s->kernels_per_step = P.nlink > 0 ? 2 : 1;
+  P.coll = d.collision;
+  P.forced = forced ? 1 : 0;
+  P.op = d.op;
+  P.om = d.om;
+  P.gx = d.accel[0];
+  P.gy = d.accel[1];
+  P.sqrt_cs2 = std::sqrt(1.0 / 3.0);
+  P.flag = s->d_flag;
+  P.bnode_idx = s->d_bidx;
+  P.bnode_first = s->d_bfirst;
+  P.nb = nb;
+  P.links = s->d_links;
+  P.pnode_idx = s->d_pidx;
+  P.pnode_n = s->d_pn;
+  P.np = (int)d.pnode_idx.size();
+  P.ctl = s->d_ctl;
+  P.ngroups = d.ngroups;
+  if (!chk(alloc_copy((void**)&s->d_partials, nullptr, (size_t)std::max(P.nlink, 1) * 2 * vl::kMaxGroups * sizeof(double))))
+    return nullptr;
+  P.partials = s->d_partials;
+  // Control block: vscale = 1, no outflow target (src/sim.rs:344-347).
+  std::memset(&s->hctl, 0, sizeof(vl::Ctl));
+  for (int g = 0; g < 4; ++g) s->hctl.vscale[g] = 1.0;
+  for (int k = 0; k < vl::kProbeCorners; ++k) s->hctl.probe_idx[k] = -1;
+  if (s->push_ctl() != VL_OK) return nullptr;
+  // Sim::from_builder ends with init to (1, 0, 0) (src/sim.rs:352).
+  if (vl_sim_init(s.get(), nullptr, nullptr, nullptr, 1.0, 0.0, 0.0) != VL_OK) return nullptr;
+  return s.release();
+}
+
+}  // namespace
+
+// ==================================================================== C ABI
+extern "C" {
+
+const char* vl_last_error(void) { return g_err.c_str(); }
+int vl_last_status(void) { return g_code; }
+int vl_abi_version(void) { return VL_ABI_VERSION; }
+int vl_set_device(int device) {
+  VL_CUDA(cudaSetDevice(device));
+  return VL_OK;
+}
+void* vl_pinned_alloc(size_t bytes) {
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+    cudaGetLastError();
+    fail(VL_ENOMEM, "cudaMallocHost failed");
+    return nullptr;
+  }
+  return p;
+}
+void vl_pinned_free(void* p) {
+  if (p) cudaFreeHost(p);
+}
+int vl_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------- shapes
+vl_shape* vl_shape_circle(double cx, double cy, double r) { return wrap_shape(std::make_unique<vl::CircleShape>(cx, cy, r)); }
+vl_shape* vl_shape_polygon(const double* xy, size_t npts) {
+  if (!xy || npts < 3) { fail(VL_EINVAL, "polygon needs at least 3 points"); return nullptr; }
+  auto p = std::make_unique<vl::PolygonShape>();
+  for (size_t k = 0; k < npts; ++k) { p->vx.push_back(xy[2 * k]); p->vy.push_back(xy[2 * k + 1]); }
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_rounded_square(double cx, double cy, double half, double r) {
+  auto p = std::make_unique<vl::RoundedSquareShape>();
+  p->cx = cx; p->cy = cy; p->half = half; p->r = r;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_rotated(vl_shape* inner, double cx, double cy, double angle) {
+  if (!inner) { fail(VL_EINVAL, "null inner shape"); return nullptr; }
+  auto p = std::make_unique<vl::RotatedShape>();
+  p->inner = std::move(inner->s); delete inner;
+  p->cx = cx; p->cy = cy; p->angle = angle;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_translated(vl_shape* inner, double dx, double dy) {
+  if (!inner) { fail(VL_EINVAL, "null inner shape"); return nullptr; }
+  auto p = std::make_unique<vl::TranslatedShape>();
+  p->inner = std::move(inner->s); delete inner;
+  p->dx = dx; p->dy = dy;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_section(int corner, double b, double cx, double cy, double d, double angle) {
+  if (corner < 0 || corner > 4) { fail(VL_EINVAL, "unknown corner kind"); return nullptr; }
+  return wrap_shape(vl::make_section(corner, b, cx, cy, d, angle));
+}
+vl_shape* vl_shape_bitmap(size_t w, size_t h, const float* level, double x0, double y0, double scale) {
+  if (!level || w == 0 || h == 0) { fail(VL_EINVAL, "empty bitmap"); return nullptr; }
+  auto p = std::make_unique<vl::BitmapShape>();
+  p->w = w; p->h = h; p->level.assign(level, level + w * h);
+  p->x0 = x0; p->y0 = y0; p->scale = scale;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_outside_band(double y0, double y1) {
+  auto p = std::make_unique<vl::OutsideBandShape>();
+  p->y0 = y0; p->y1 = y1;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_ellipse(double cx, double cy, double a, double b) {
+  if (!(a > 0.0 && b > 0.0)) { fail(VL_EINVAL, "ellipse semi-axes must be positive"); return nullptr; }
+  auto p = std::make_unique<vl::EllipseShape>();
+  p->cx = cx; p->cy = cy; p->a = a; p->b = b;
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_disks(const double* cxcyr, size_t ndisks) {
+  if (!cxcyr || ndisks == 0) { fail(VL_EINVAL, "disk union needs at least one disk"); return nullptr; }
+  auto p = std::make_unique<vl::DiskUnionShape>();
+  for (size_t k = 0; k < ndisks; ++k) {
+    p->cx.push_back(cxcyr[3 * k]);
+    p->cy.push_back(cxcyr[3 * k + 1]);
+    p->r.push_back(cxcyr[3 * k + 2]);
+  }
+  p->index();
+  return wrap_shape(std::move(p));
+}
+vl_shape* vl_shape_star(double cx, double cy, const double* radii, size_t nvert, double phase) {
+  if (!radii || nvert < 3) { fail(VL_EINVAL, "star polygon needs at least 3 vertices"); return nullptr; }
+  return wrap_shape(vl::make_star(cx, cy, radii, nvert, phase));
+}
+void vl_shape_free(vl_shape* s) { delete s; }
+int vl_shape_inside(const vl_shape* s, double x, double y) { return s && s->s->inside(x, y) ? 1 : 0; }
+double vl_cut_fraction(const vl_shape* s, double x, double y, double dx, double dy) {
+  return s ? vl::cut_fraction(*s->s, x, y, dx, dy) : std::nan("");
+}
+int vl_bounding_box(const vl_shape* s, double reach, double step, double* out) {
+  if (!s || !out || !(step > 0.0)) return fail(VL_EINVAL, "bounding_box: bad arguments");
+  return vl::bounding_box(*s->s, reach, step, out) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- builder
+vl_builder* vl_builder_new(size_t nx, size_t ny) {
+  if (nx < 3 || ny < 3) { fail(VL_EINVAL, "grid must be at least 3 x 3"); return nullptr; }
+  auto b = new vl_builder();
+  b->spec.nx = nx;
+  b->spec.ny = ny;
+  b->spec.kinds.emplace_back();
+  b->spec.paint.assign(nx * ny, 0);
+  return b;
+}
+void vl_builder_free(vl_builder* b) { delete b; }
+int vl_builder_set_periodic(vl_builder* b, int px, int py) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  b->spec.periodic_x = px != 0;
+  b->spec.periodic_y = py != 0;
+  return VL_OK;
+}
+int vl_builder_set_tau(vl_builder* b, double tau) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  b->spec.tau = tau;
+  return VL_OK;
+}
+int vl_builder_set_collision(vl_builder* b, int collision, double magic) {
+  if (!b || (collision != VL_BGK && collision != VL_TRT)) return fail(VL_EINVAL, "bad collision model");
+  b->spec.collision = collision;
+  b->spec.magic = magic;
+  return VL_OK;
+}
+int vl_builder_set_accel(vl_builder* b, double gx, double gy) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  b->spec.accel[0] = gx;
+  b->spec.accel[1] = gy;
+  return VL_OK;
+}
+static int add_kind(vl_builder* b, vl::CellKind&& k) {
+  if (b->spec.kinds.size() >= 255) return fail(VL_EINVAL, "at most 254 cell kinds (src/sim.rs:101)");
+  b->spec.kinds.push_back(std::move(k));
+  return (int)b->spec.kinds.size() - 1;
+}
+int vl_builder_add_wall(vl_builder* b, const vl_wall* w) {
+  std::unique_ptr<vl::Shape> shape;
+  if (w && w->shape) { shape = std::move(w->shape->s); delete w->shape; }
+  if (!b || !w) return fail(VL_EINVAL, "null builder or wall");
+  if (w->vgroup < 0 || w->vgroup >= VL_VGROUPS) return fail(VL_EINVAL, "vgroup must be below 4 (src/sim.rs:303)");
+  if (w->fgroup >= VL_MAX_FGROUPS) return fail(VL_EINVAL, "force group must be below VL_MAX_FGROUPS (4)");
+  if (w->velocity.kind < VL_VEL_NONE || w->velocity.kind > VL_VEL_ROTATION) return fail(VL_EINVAL, "unknown velocity kind");
+  vl::CellKind k;
+  k.tag = vl::KIND_WALL;
+  k.velocity.kind = w->velocity.kind;
+  for (int i = 0; i < 4; ++i) k.velocity.p[i] = w->velocity.p[i];
+  k.vgroup = w->vgroup;
+  k.fgroup = w->fgroup < 0 ? -1 : w->fgroup;
+  k.shape = std::move(shape);
+  return add_kind(b, std::move(k));
+}
+int vl_builder_add_static_wall(vl_builder* b) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  vl::CellKind k;
+  k.tag = vl::KIND_WALL;
+  return add_kind(b, std::move(k));
+}
+int vl_builder_add_pressure(vl_builder* b, double rho) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  vl::CellKind k;
+  k.tag = vl::KIND_PRESSURE;
+  k.rho = rho;
+  return add_kind(b, std::move(k));
+}
+int vl_builder_add_radiating(vl_builder* b, double rho) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  vl::CellKind k;
+  k.tag = vl::KIND_RADIATING;
+  k.rho = rho;
+  return add_kind(b, std::move(k));
+}
+int vl_builder_fill_rect(vl_builder* b, size_t x0, size_t x1, size_t y0, size_t y1, int kind) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  if (kind < 0 || (size_t)kind >= b->spec.kinds.size()) return fail(VL_EINVAL, "unknown kind");
+  if (x1 >= b->spec.nx || y1 >= b->spec.ny) return fail(VL_EINVAL, "rectangle outside the grid");
+  for (size_t y = y0; y <= y1; ++y)
+    for (size_t x = x0; x <= x1; ++x) b->spec.paint[y * b->spec.nx + x] = (uint8_t)kind;
+  return VL_OK;
+}
+int vl_builder_fill_shape(vl_builder* b, int kind) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  if (kind < 0 || (size_t)kind >= b->spec.kinds.size()) return fail(VL_EINVAL, "unknown kind");
+  const vl::CellKind& k = b->spec.kinds[kind];
+  if (k.tag != vl::KIND_WALL || !k.shape) return fail(VL_EINVAL, "fill_shape needs a wall kind with an outline");
+  for (size_t y = 0; y < b->spec.ny; ++y)
+    for (size_t x = 0; x < b->spec.nx; ++x)
+      if (k.shape->inside((double)x, (double)y)) b->spec.paint[y * b->spec.nx + x] = (uint8_t)kind;
+  return VL_OK;
+}
+int vl_builder_link_table(vl_builder* b, size_t* nlinks, size_t* nbnodes, size_t* npnodes, uint8_t* flags,
+                          int32_t* bnode_idx, int32_t* bnode_first, double* link_f64, int32_t* link_i32) {
+  if (!b || !nlinks || !nbnodes || !npnodes) return fail(VL_EINVAL, "null argument");
+  vl::CompiledDomain dom;
+  std::string err;
+  if (!vl::compile_domain(b->spec, dom, err)) return fail(VL_EINVAL, err);
+  *nlinks = dom.links.size();
+  *nbnodes = dom.bnode_idx.size();
+  *npnodes = dom.pnode_idx.size();
+  if (flags) std::memcpy(flags, dom.flag.data(), dom.n);
+  if (bnode_idx) std::memcpy(bnode_idx, dom.bnode_idx.data(), dom.bnode_idx.size() * 4);
+  if (bnode_first) std::memcpy(bnode_first, dom.bnode_first.data(), dom.bnode_first.size() * 4);
+  for (size_t k = 0; k < dom.links.size(); ++k) {
+    const vl::LinkRec& L = dom.links[k];
+    if (link_f64) {
+      double* o = link_f64 + 5 * k;
+      o[0] = L.q; o[1] = L.cu6; o[2] = L.uw[0]; o[3] = L.uw[1]; o[4] = L.rho;
+    }
+    if (link_i32) {
+      int32_t* o = link_i32 + 7 * k;
+      o[0] = L.dir; o[1] = L.flags & 1; o[2] = (L.flags >> 1) & 1; o[3] = L.vgroup; o[4] = L.fgroup;
+      o[5] = L.behind; o[6] = ((L.flags >> 2) & 3) - 1 + 3 * (((L.flags >> 4) & 3) - 1 + 1) + 1;
+    }
+  }
+  return VL_OK;
+}
+
+vl_sim* vl_builder_build(vl_builder* b, int precision) {
+  if (!b) { fail(VL_EINVAL, "null builder"); return nullptr; }
+  std::unique_ptr<vl_builder> own(b);
+  vl::CompiledDomain dom;
+  std::string err;
+  if (!vl::compile_domain(b->spec, dom, err)) { fail(VL_EINVAL, err); return nullptr; }
+  return make_sim(std::move(dom), precision);
+}
+
+// ---------------------------------------------------------------- sim
+void vl_sim_free(vl_sim* s) { delete s; }
+
+int vl_sim_info(const vl_sim* s, size_t* nx, size_t* ny, size_t* fluid, size_t* nlinks, size_t* nbn, int* ngroups,
+                int* prec) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  if (nx) *nx = s->dom.nx;
+  if (ny) *ny = s->dom.ny;
+  if (fluid) *fluid = s->dom.fluid_nodes;
+  if (nlinks) *nlinks = s->dom.links.size();
+  if (nbn) *nbn = s->dom.bnode_idx.size();
+  if (ngroups) *ngroups = s->dom.ngroups;
+  if (prec) *prec = s->prec;
+  return VL_OK;
+}
+
+int vl_sim_init(vl_sim* s, const double* rho, const double* ux, const double* uy, double rho0, double ux0, double uy0) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  if ((rho || ux || uy) && !(rho && ux && uy)) return fail(VL_EINVAL, "init: give all three field arrays or none");
+  VL_CUDA(cudaSetDevice(s->device));
+  double* d_field = nullptr;
+  const size_t n = s->n;
+  if (rho) {
+    VL_CUDA(cudaMalloc(&d_field, 3 * n * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(d_field, rho, n * 8, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_field + n, ux, n * 8, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_field + 2 * n, uy, n * 8, cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) { cudaFree(d_field); return cuda_fail(e, "init upload"); }
+  }
+  cudaError_t e = s->L->init((int)n, s->ns, s->d_flag, d_field, d_field ? d_field + n : nullptr,
+                             d_field ? d_field + 2 * n : nullptr, rho0, ux0, uy0, s->buf[0], s->buf[1], s->stream);
+  if (d_field) {
+    cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    cudaFree(d_field);
+    if (e == cudaSuccess) e = e2;
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "init");
+  // t = 0 (src/sim.rs:370); the force and the outlet offset restart from zero.
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  s->hctl.t = 0;
+  s->hctl.arrive = 0;
+  s->hctl.nonfinite = 0;
+  s->hctl.nonfinite_t = 0;
+  s->hctl.drho = 0.0;
+  for (int k = 0; k < 2 * vl::kMaxGroups; ++k) s->hctl.force[k] = 0.0;
+  s->t_host = 0;
+  if (s->rec_cap) s->hctl.rec_start = 0;
+  s->rec_start = 0;
+  return s->push_ctl();
+}
+
+int vl_sim_step(vl_sim* s, uint64_t steps) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  return s->step(steps);
+}
+
+int vl_sim_synchronize(vl_sim* s) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  VL_CUDA(cudaStreamSynchronize(s->stream));
+  return VL_OK;
+}
+
+int vl_sim_set_vscale(vl_sim* s, int g, double v) {
+  if (!s || g < 0 || g >= VL_VGROUPS) return fail(VL_EINVAL, "vscale group out of range");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  s->hctl.vscale[g] = v;
+  return s->push_ctl();
+}
+
+int vl_sim_get_vscale(const vl_sim* cs, double* out4) {
+  vl_sim* s = const_cast<vl_sim*>(cs);
+  if (!s || !out4) return fail(VL_EINVAL, "null argument");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  for (int g = 0; g < 4; ++g) out4[g] = s->hctl.vscale[g];
+  return VL_OK;
+}
+
+int vl_sim_set_outflow_target(vl_sim* s, int enabled, double target) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  s->hctl.has_target = enabled ? 1 : 0;
+  s->hctl.target = target;
+  return s->push_ctl();
+}
+
+int vl_sim_outlet_density_offset(vl_sim* s, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  *out = s->hctl.drho;
+  return VL_OK;
+}
+
+int vl_sim_t(vl_sim* s, uint64_t* t) {
+  if (!s || !t) return fail(VL_EINVAL, "null argument");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  *t = s->hctl.t;
+  return VL_OK;
+}
+
+int vl_sim_force(vl_sim* s, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  for (int k = 0; k < 2 * s->dom.ngroups; ++k) out[k] = s->hctl.force[k];
+  return VL_OK;
+}
+
+int vl_sim_status(vl_sim* s, int* nonfinite, uint64_t* first_t) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  if (nonfinite) *nonfinite = s->hctl.nonfinite;
+  if (first_t) *first_t = s->hctl.nonfinite_t;
+  return VL_OK;
+}
+
+int vl_sim_download(vl_sim* s, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  VL_CUDA(cudaSetDevice(s->device));
+  const size_t n = s->n;
+  if (s->prec == VL_F64) {
+    VL_CUDA(cudaMemcpy2DAsync(out, n * 8, s->a(), (size_t)s->ns * 8, n * 8, 9, cudaMemcpyDeviceToHost, s->stream));
+  } else {
+    double* tmp = nullptr;
+    VL_CUDA(cudaMalloc(&tmp, 9 * n * sizeof(double)));
+    cudaError_t e = s->L->to_f64((int)n, s->ns, s->a(), tmp, s->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, 9 * n * 8, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "download");
+  }
+  VL_CUDA(cudaStreamSynchronize(s->stream));
+  return VL_OK;
+}
+
+int vl_sim_upload(vl_sim* s, const double* in) {
+  if (!s || !in) return fail(VL_EINVAL, "null argument");
+  VL_CUDA(cudaSetDevice(s->device));
+  const size_t n = s->n;
+  if (s->prec == VL_F64) {
+    VL_CUDA(cudaMemcpy2DAsync(s->buf[s->cur], (size_t)s->ns * 8, in, n * 8, n * 8, 9, cudaMemcpyHostToDevice, s->stream));
+  } else {
+    double* tmp = nullptr;
+    VL_CUDA(cudaMalloc(&tmp, 9 * n * sizeof(double)));
+    cudaError_t e = cudaMemcpyAsync(tmp, in, 9 * n * 8, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = s->L->from_f64((int)n, s->ns, tmp, s->buf[s->cur], s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_fail(e, "upload");
+  }
+  VL_CUDA(cudaStreamSynchronize(s->stream));
+  return VL_OK;
+}
+
+int vl_sim_flags(vl_sim* s, uint8_t* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  std::memcpy(out, s->dom.flag.data(), s->n);
+  return VL_OK;
+}
+
+int vl_sim_macros_field(vl_sim* s, double* rho, double* ux, double* uy) {
+  if (!s || !rho || !ux || !uy) return fail(VL_EINVAL, "null argument");
+  VL_CUDA(cudaSetDevice(s->device));
+  const size_t n = s->n;
+  double* tmp = nullptr;
+  VL_CUDA(cudaMalloc(&tmp, 3 * n * sizeof(double)));
+  cudaError_t e = s->L->macros((int)n, s->ns, s->d_flag, s->dom.accel[0], s->dom.accel[1], s->a(), tmp, tmp + n,
+                               tmp + 2 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rho, tmp, n * 8, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ux, tmp + n, n * 8, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(uy, tmp + 2 * n, n * 8, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(e, "macros_field");
+  return VL_OK;
+}
+
+int vl_sim_macros(vl_sim* s, size_t x, size_t y, double* out3) {
+  if (!s || !out3 || x >= s->dom.nx || y >= s->dom.ny) return fail(VL_EINVAL, "macros: bad arguments");
+  const size_t idx = y * s->dom.nx + x;
+  if (s->dom.flag[idx] == 2) { out3[0] = 1.0; out3[1] = 0.0; out3[2] = 0.0; return VL_OK; }
+  std::vector<double> f;
+  int rc = s->gather({(int32_t)idx}, f);
+  if (rc) return rc;
+  double rho, jx, jy;
+  moments_host(f.data(), rho, jx, jy);
+  out3[0] = rho;
+  out3[1] = jx / rho - 0.5 * s->dom.accel[0];
+  out3[2] = jy / rho - 0.5 * s->dom.accel[1];
+  return VL_OK;
+}
+
+static int sim_reduce(vl_sim* s, double* mass, double* mom, double* vmax) {
+  VL_CUDA(cudaSetDevice(s->device));
+  cudaError_t e = s->L->reduce((int)s->n, s->ns, s->d_flag, s->dom.accel[0], s->dom.accel[1], s->a(), s->d_red,
+                               kReduceBlocks, s->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "reduce");
+  std::vector<double> r(kReduceBlocks * 7);
+  VL_CUDA(cudaMemcpyAsync(r.data(), s->d_red, r.size() * 8, cudaMemcpyDeviceToHost, s->stream));
+  VL_CUDA(cudaStreamSynchronize(s->stream));
+  // Fixed-order combination of the per-block compensated sums.
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  double vm = 0.0;
+  bool nan = false;
+  for (int b = 0; b < kReduceBlocks; ++b) {
+    const double* o = &r[7 * b];
+    for (int k = 0; k < 3; ++k) {
+      double& sum = acc[2 * k];
+      double& comp = acc[2 * k + 1];
+      const double x = o[2 * k];
+      const double t = sum + x;
+      comp += std::fabs(sum) >= std::fabs(x) ? (sum - t) + x : (x - t) + sum;
+      sum = t;
+      comp += o[2 * k + 1];
+    }
+    if (std::isnan(o[6])) nan = true; else vm = std::fmax(vm, o[6]);
+  }
+  if (mass) *mass = acc[0] + acc[1];
+  if (mom) { mom[0] = acc[2] + acc[3]; mom[1] = acc[4] + acc[5]; }
+  if (vmax) *vmax = nan ? std::nan("") : vm;
+  return VL_OK;
+}
+
+int vl_sim_total_mass(vl_sim* s, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  return sim_reduce(s, out, nullptr, nullptr);
+}
+int vl_sim_total_momentum(vl_sim* s, double* out2) {
+  if (!s || !out2) return fail(VL_EINVAL, "null argument");
+  return sim_reduce(s, nullptr, out2, nullptr);
+}
+int vl_sim_max_speed(vl_sim* s, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  return sim_reduce(s, nullptr, nullptr, out);
+}
+
+// Sim::vorticity (src/sim.rs:582-620): central differences, one-sided next to solids.
+int vl_sim_vorticity(vl_sim* s, float* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  const size_t nx = s->dom.nx, ny = s->dom.ny, n = s->n;
+  std::vector<double> rho(n), ux(n), uy(n);
+  int rc = vl_sim_macros_field(s, rho.data(), ux.data(), uy.data());
+  if (rc) return rc;
+  for (size_t k = 0; k < n; ++k) {
+    out[k] = 0.0f;
+    if (s->dom.flag[k] == 2) { ux[k] = 0.0; uy[k] = 0.0; }
+  }
+  auto fluid = [&](long x, long y) {
+    return x >= 0 && y >= 0 && x < (long)nx && y < (long)ny && s->dom.flag[(size_t)y * nx + (size_t)x] != 2;
+  };
+  auto get = [&](long x, long y, int comp) {
+    const size_t k = (size_t)y * nx + (size_t)x;
+    return comp == 0 ? ux[k] : uy[k];
+  };
+  for (long y = 0; y < (long)ny; ++y) {
+    for (long x = 0; x < (long)nx; ++x) {
+      if (!fluid(x, y)) continue;
+      auto diff = [&](long dx, long dy, int comp) -> double {
+        const bool p = fluid(x + dx, y + dy), m = fluid(x - dx, y - dy);
+        if (p && m) return 0.5 * (get(x + dx, y + dy, comp) - get(x - dx, y - dy, comp));
+        if (p) return get(x + dx, y + dy, comp) - get(x, y, comp);
+        if (m) return get(x, y, comp) - get(x - dx, y - dy, comp);
+        return 0.0;
+      };
+      out[(size_t)y * nx + (size_t)x] = (float)(diff(1, 0, 1) - diff(0, 1, 0));
+    }
+  }
+  return VL_OK;
+}
+
+int vl_sim_probe_density(vl_sim* s, double x, double y, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  return sim_probe_density(s, x, y, out);
+}
+
+int vl_sim_probe_density_at_wall(vl_sim* s, double x, double y, double nx, double ny, double* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  double p[3];
+  for (int d = 1; d <= 3; ++d) {
+    int rc = sim_probe_density(s, x + (double)d * nx, y + (double)d * ny, &p[d - 1]);
+    if (rc) return rc;
+  }
+  *out = 3.0 * p[0] - 3.0 * p[1] + p[2];
+  return VL_OK;
+}
+
+// FNV-1a over the little-endian bytes of every fluid population, cell-major (src/sim.rs:654-668).
+int vl_sim_state_hash(vl_sim* s, uint64_t* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  const size_t n = s->n;
+  std::vector<double> f(9 * n);
+  int rc = vl_sim_download(s, f.data());
+  if (rc) return rc;
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (size_t idx = 0; idx < n; ++idx) {
+    if (s->dom.flag[idx] == 2) continue;
+    for (int i = 0; i < 9; ++i) {
+      uint64_t bits;
+      std::memcpy(&bits, &f[(size_t)i * n + idx], 8);
+      for (int k = 0; k < 8; ++k) {
+        h ^= (bits >> (8 * k)) & 0xffu;
+        h *= 0x100000001b3ull;
+      }
+    }
+  }
+  *out = h;
+  return VL_OK;
+}
+
+int vl_sim_record(vl_sim* s, uint64_t capacity) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  VL_CUDA(cudaSetDevice(s->device));
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  if (capacity > s->rec_cap || capacity == 0) {
+    if (s->d_hist) { cudaFree(s->d_hist); s->d_hist = nullptr; }
+    if (capacity) VL_CUDA(cudaMalloc(&s->d_hist, capacity * vl::kRec * sizeof(double)));
+  }
+  s->rec_cap = capacity;
+  s->rec_start = s->hctl.t;
+  s->hctl.hist = s->d_hist;
+  s->hctl.rec_cap = capacity;
+  s->hctl.rec_start = s->hctl.t;
+  return s->push_ctl();
+}
+
+int vl_sim_history(vl_sim* s, double* out, uint64_t* count) {
+  if (!s || !count) return fail(VL_EINVAL, "null argument");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  uint64_t have = s->hctl.t >= s->hctl.rec_start ? s->hctl.t - s->hctl.rec_start : 0;
+  have = std::min(have, s->rec_cap);
+  if (out && have) {
+    VL_CUDA(cudaMemcpyAsync(out, s->d_hist, have * vl::kRec * sizeof(double), cudaMemcpyDeviceToHost, s->stream));
+    VL_CUDA(cudaStreamSynchronize(s->stream));
+  }
+  *count = have;
+  return VL_OK;
+}
+
+int vl_sim_set_dp_probe(vl_sim* s, double xc, double yc, double r, double u_ref) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  int rc = s->pull_ctl();
+  if (rc) return rc;
+  // Front wall point (xc - r, yc) with outward normal (-1, 0), back (xc + r, yc) with (1, 0);
+  // samples at distances 1, 2, 3 (src/sim.rs:648-651, src/cases/cylinder.rs:272-277).
+  const double wx[2] = {xc - r, xc + r}, nxv[2] = {-1.0, 1.0};
+  for (int side = 0; side < 2; ++side)
+    for (int d = 0; d < 3; ++d) {
+      const int base = (side * 3 + d) * 4;
+      probe_corners(*s, wx[side] + (double)(d + 1) * nxv[side], yc + (double)(d + 1) * 0.0, &s->hctl.probe_idx[base],
+                    &s->hctl.probe_w[base]);
+    }
+  s->hctl.dp_on = 1;
+  s->hctl.u_ref = u_ref;
+  return s->push_ctl();
+}
+
+int vl_sim_last_step_ms(vl_sim* s, float* ms) {
+  if (!s || !ms) return fail(VL_EINVAL, "null argument");
+  if (!s->timed) return fail(VL_EINVAL, "no step batch timed yet");
+  VL_CUDA(cudaEventSynchronize(s->ev1));
+  VL_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
+  return VL_OK;
+}
+
+int vl_sim_step_profiled(vl_sim* s, uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms) {
+  if (!s || steps == 0) return fail(VL_EINVAL, "step_profiled: bad arguments");
+  return s->step_profiled(steps, link_ms, bulk_ms, total_ms);
+}
+
+int vl_sim_launch_count(vl_sim* s, uint64_t* out) {
+  if (!s || !out) return fail(VL_EINVAL, "null argument");
+  *out = s->launches;
+  return VL_OK;
+}
+
+// ---------------------------------------------------------------- channel (src/cases/channel.rs)
+}  // extern "C"
+
+struct vl_channel {
+  vl_sim* sim = nullptr;
+  double u_ref = 0.0;
+  uint64_t ramp_steps = 0;
+  ~vl_channel() { delete sim; }
+};
+
+extern "C" {
+
+vl_channel* vl_channel_new(const vl_channel_spec* sp, int precision) {
+  if (!sp) { fail(VL_EINVAL, "null spec"); return nullptr; }
+  std::unique_ptr<vl::Shape> body;
+  if (sp->body) { body = std::move(sp->body->s); delete sp->body; }
+  if (!body) { fail(VL_EINVAL, "channel needs a body shape"); return nullptr; }
+  const size_t nx = sp->nx, ny = sp->ny;
+  if (nx < 3 || ny < 3) { fail(VL_EINVAL, "grid must be at least 3 x 3"); return nullptr; }
+  if (sp->inflow < 0 || sp->inflow > 2) { fail(VL_EINVAL, "unknown inflow"); return nullptr; }
+  // Channel::new (src/cases/channel.rs:71-116): inlet (moving wall, vgroup 1) at x = 0, outlet
+  // (pressure 1) at x = nx-1, side walls, body (vgroup 2, force group 0).
+  const double h = (double)(ny - 2);
+  vl::DomainSpec spec;
+  spec.nx = nx;
+  spec.ny = ny;
+  spec.tau = vl_tau_for(sp->nu);
+  spec.collision = sp->collision;
+  spec.magic = sp->magic;
+  spec.kinds.emplace_back();
+  spec.paint.assign(nx * ny, 0);
+  vl::WallVelocity profile;
+  if (sp->inflow == VL_INFLOW_PARABOLIC) { profile.kind = vl::VEL_PARABOLIC; profile.p[0] = sp->u; profile.p[1] = h; }
+  else { profile.kind = vl::VEL_CONST; profile.p[0] = sp->u; }
+  auto add = [&](vl::CellKind&& k) {
+    spec.kinds.push_back(std::move(k));
+    return (uint8_t)(spec.kinds.size() - 1);
+  };
+  auto fill = [&](size_t x0, size_t x1, size_t y0, size_t y1, uint8_t k) {
+    for (size_t y = y0; y <= y1; ++y)
+      for (size_t x = x0; x <= x1; ++x) spec.paint[y * nx + x] = k;
+  };
+  vl::CellKind inlet;
+  inlet.tag = vl::KIND_WALL;
+  inlet.velocity = profile;
+  inlet.vgroup = 1;
+  const uint8_t k_in = add(std::move(inlet));
+  vl::CellKind outlet;
+  outlet.tag = vl::KIND_PRESSURE;
+  outlet.rho = 1.0;
+  const uint8_t k_out = add(std::move(outlet));
+  vl::CellKind walls;
+  if (sp->inflow == VL_INFLOW_PARABOLIC) walls.tag = vl::KIND_WALL;
+  else if (sp->inflow == VL_INFLOW_UNIFORM) {
+    walls.tag = vl::KIND_WALL;
+    walls.velocity.kind = vl::VEL_CONST;
+    walls.velocity.p[0] = sp->u;
+    walls.vgroup = 1;
+  } else {
+    walls.tag = vl::KIND_RADIATING;
+    walls.rho = 1.0;
+  }
+  const uint8_t k_w = add(std::move(walls));
+  fill(0, 0, 0, ny - 1, k_in);
+  fill(nx - 1, nx - 1, 0, ny - 1, k_out);
+  fill(1, nx - 2, 0, 0, k_w);
+  fill(1, nx - 2, ny - 1, ny - 1, k_w);
+  if (sp->inflow != VL_INFLOW_UNIFORM_OPEN) {
+    fill(0, nx - 1, 0, 0, k_w);
+    fill(0, nx - 1, ny - 1, ny - 1, k_w);
+  }
+  vl::CellKind bk;
+  bk.tag = vl::KIND_WALL;
+  bk.vgroup = 2;
+  bk.fgroup = 0;
+  if (sp->has_kick) { bk.velocity.kind = vl::VEL_ROTATION; bk.velocity.p[0] = sp->kick_cx; bk.velocity.p[1] = sp->kick_cy; }
+  bk.shape = std::move(body);
+  const uint8_t k_b = add(std::move(bk));
+  {
+    const vl::Shape& shape = *spec.kinds[k_b].shape;
+    for (size_t y = 0; y < ny; ++y)
+      for (size_t x = 0; x < nx; ++x)
+        if (shape.inside((double)x, (double)y)) spec.paint[y * nx + x] = k_b;
+  }
+  vl::CompiledDomain dom;
+  std::string err;
+  if (!vl::compile_domain(spec, dom, err)) { fail(VL_EINVAL, err); return nullptr; }
+  vl_sim* sim = make_sim(std::move(dom), precision);
+  if (!sim) return nullptr;
+  auto ch = std::make_unique<vl_channel>();
+  ch->sim = sim;
+  ch->u_ref = sp->u;
+  ch->ramp_steps = sp->ramp_steps;
+  if (sp->ramp_steps == 0) {
+    // Start from the developed inflow profile (src/cases/channel.rs:108-110).
+    std::vector<double> rho(sim->n, 1.0), ux(sim->n), uy(sim->n, 0.0);
+    for (size_t y = 0; y < ny; ++y) {
+      double u, v;
+      profile.at(0.0, (double)y, u, v);
+      for (size_t x = 0; x < nx; ++x) ux[y * nx + x] = u;
+    }
+    if (vl_sim_init(sim, rho.data(), ux.data(), uy.data(), 1.0, 0.0, 0.0) != VL_OK) return nullptr;
+  }
+  // Per-step controls (src/cases/channel.rs:118-130): inlet ramp and body kick, precomputed for
+  // every step until both are constant (ramp 1, kick 0), then uploaded once.
+  uint64_t len = sp->ramp_steps;
+  if (sp->has_kick) len = std::max<uint64_t>(len, sp->kick_start + sp->kick_duration);
+  std::vector<double> sched(2 * std::max<uint64_t>(len, 1));
+  for (uint64_t t = 0; t < len; ++t) {
+    sched[2 * t] = vl_ramp(t, sp->ramp_steps);
+    double v2 = 0.0;
+    if (sp->has_kick && t >= sp->kick_start && t < sp->kick_start + sp->kick_duration) {
+      const double s = (double)(t - sp->kick_start) / (double)sp->kick_duration;
+      const double a = std::sin(M_PI * s);
+      v2 = sp->kick_omega * (a * a) * std::copysign(1.0, std::sin(2.0 * M_PI * s));
+    }
+    sched[2 * t + 1] = v2;
+  }
+  if (cudaMalloc(&sim->d_sched, sched.size() * sizeof(double)) != cudaSuccess ||
+      cudaMemcpy(sim->d_sched, sched.data(), sched.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+    fail(VL_ECUDA, "schedule upload");
+    return nullptr;
+  }
+  if (sim->pull_ctl() != VL_OK) return nullptr;
+  sim->hctl.sched_on = 1;
+  sim->hctl.sched = sim->d_sched;
+  sim->hctl.sched_len = len;
+  sim->hctl.u_ref = sp->u;
+  sim->hctl.absorbing = 1;
+  if (sim->push_ctl() != VL_OK) return nullptr;
+  return ch.release();
+}
+
+void vl_channel_free(vl_channel* c) { delete c; }
+vl_sim* vl_channel_sim(vl_channel* c) { return c ? c->sim : nullptr; }
+double vl_channel_u_ref(const vl_channel* c) { return c ? c->u_ref : std::nan(""); }
+
+int vl_channel_set_absorbing(vl_channel* c, int on) {
+  if (!c) return fail(VL_EINVAL, "null channel");
+  int rc = c->sim->pull_ctl();
+  if (rc) return rc;
+  c->sim->hctl.absorbing = on ? 1 : 0;
+  return c->sim->push_ctl();
+}
+
+int vl_channel_step(vl_channel* c, uint64_t steps) {
+  if (!c) return fail(VL_EINVAL, "null channel");
+  return c->sim->step(steps);
+}
+
+int vl_channel_coefficients(vl_channel* c, double d, double* cd, double* cl) {
+  if (!c || !cd || !cl) return fail(VL_EINVAL, "null argument");
+  double f[2 * VL_MAX_FGROUPS] = {0};
+  int rc = vl_sim_force(c->sim, f);
+  if (rc) return rc;
+  const double k = 2.0 / (c->u_ref * c->u_ref * d);
+  *cd = k * f[0];
+  *cl = k * f[1];
+  return VL_OK;
+}
+
+// ---------------------------------------------------------------- signal / small helpers
+int vl_fft(double* re, double* im, size_t n) {
+  if (!re || !im || n == 0 || (n & (n - 1))) return fail(VL_EINVAL, "FFT length must be a power of two");
+  vl::fft_inplace(re, im, n);
+  return VL_OK;
+}
+double vl_mean(const double* x, size_t n) { return vl::series_mean(x, n); }
+double vl_rms(const double* x, size_t n) { return vl::series_rms(x, n); }
+int vl_dominant_frequency(const double* x, size_t n, double dt, double* freq, double* amp) {
+  if (!x || n < 2 || !freq || !amp) return fail(VL_EINVAL, "dominant_frequency: bad arguments");
+  vl::dominant_frequency(x, n, dt, *freq, *amp);
+  return VL_OK;
+}
+size_t vl_peaks(const double* x, size_t n, double* pos, double* val, size_t cap) {
+  return x ? vl::find_peaks(x, n, pos, val, cap) : 0;
+}
+int vl_crossing_frequency(const double* x, size_t n, double dt, double* out) {
+  if (!x || !out) return fail(VL_EINVAL, "null argument");
+  return vl::crossing_frequency(x, n, dt, *out) ? 1 : 0;
+}
+double vl_sample_at(const double* x, size_t n, double pos) { return (x && n >= 2) ? vl::sample_at(x, n, pos) : std::nan(""); }
+double vl_ramp(uint64_t t, uint64_t steps) {
+  if (steps == 0 || t >= steps) return 1.0;
+  const double s = (double)t / (double)steps;
+  return s * s * (3.0 - 2.0 * s);
+}
+double vl_tau_for(double nu) { return nu / (1.0 / 3.0) + 0.5; }
+
+}  // extern "C"

@@ -1,0 +1,602 @@
+// Device data structures and the step kernels (templated on storage and arithmetic type).
+//
+// One time step of the reference (src/sim.rs:391-420) is two kernels on one stream:
+//
+//   k_links  boundary nodes: gather the 9 incoming populations, replace every population that
+//            would come out of a wall or open boundary with the boundary rule of its link
+//            (src/sim.rs:456-507), accumulate the momentum-exchange force per force group,
+//            collide, write. One thread per boundary node, grid-stride over the CSR node list.
+//   k_bulk   interior nodes (flag 0): pull the 9 populations from the upstream neighbours with
+//            periodic wrap (src/sim.rs:700-735), collide, write. One thread per cell of a
+//            row tile, grid-stride over tiles.
+//
+// Both read only `a` and write disjoint cells of `b`, so their order does not matter; the
+// whole-step epilogue runs in whichever block of the two launches arrives last (a counter in
+// device memory, no spin-waits): it reduces the per-block force partials in a fixed order, writes
+// the per-step record, evaluates the pressure-drop probes on the new state and advances t.
+//
+// Determinism: every population update is a pure function of `a`; the force is summed per thread
+// in link order, then by a fixed warp-shuffle tree, a fixed shared-memory tree and a fixed tree
+// over block partials, so runs are bit-identical run to run. The outlet density offset
+// (src/sim.rs:444-455) is a sequential sum in pnode order, as in the reference.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "vl_lattice.hpp"
+
+namespace vl {
+
+constexpr int kBlock = 256;       // threads per block for both step kernels
+constexpr int kMaxGroups = 4;     // force groups
+constexpr int kRec = 10;          // doubles per history record
+constexpr int kProbeCorners = 24; // 2 wall points x 3 distances x 4 cells
+
+// Device-resident control block of one sim. Written by the host between batches (stream-ordered
+// copies) and by the step epilogue.
+struct Ctl {
+  double vscale[4];
+  double target;
+  double drho;                 // outlet density offset used in the last step
+  double force[2 * kMaxGroups];
+  unsigned long long t;
+  unsigned long long rec_start;  // t of history record 0
+  unsigned long long rec_cap;    // records available (0 = not recording)
+  unsigned long long nonfinite_t;
+  unsigned int arrive;         // blocks of the current step that have finished
+  int has_target;
+  int nonfinite;               // set once a non-finite force is seen
+  int sched_on;                // channel mode: controls from the schedule below
+  int absorbing;
+  int dp_on;
+  double u_ref;
+  unsigned long long sched_len;
+  const double* sched;         // [sched_len][2] = (inlet ramp, body kick) per step
+  double* hist;                // [rec_cap][kRec]
+  // pressure-drop probe: per (side, distance) the valid corner cells and bilinear weights
+  int probe_idx[kProbeCorners];  // -1: corner skipped (outside, solid or zero weight)
+  double probe_w[kProbeCorners];
+};
+
+struct StepParams {
+  int nx, ny;
+  unsigned ns;                 // population plane stride (elements)
+  int tiles_per_row, ntiles;   // bulk tiling: one tile = kBlock consecutive cells of a row
+  int nbulk, nlink;            // blocks in each launch
+  int coll, forced;
+  double op, om, gx, gy;
+  double sqrt_cs2;
+  const uint8_t* flag;
+  const int32_t* bnode_idx;
+  const int32_t* bnode_first;  // nb + 1 entries
+  int nb;
+  const void* links;           // LinkRecDev[]
+  const int32_t* pnode_idx;
+  const int8_t* pnode_n;       // (nx, ny) pairs
+  int np;
+  Ctl* ctl;
+  double* partials;            // [nlink][2 * kMaxGroups]
+  int ngroups;
+};
+
+struct alignas(16) LinkRecDev {
+  double q, cu6, uw0, uw1, rho;
+  int32_t behind;
+  uint8_t dir, flags, vgroup;
+  int8_t fgroup;
+};
+static_assert(sizeof(LinkRecDev) == 48, "link record");
+
+// ------------------------------------------------------------------ storage traits
+// S = stored type, R = arithmetic type. FP16 storage keeps f_i - w_i (the shifted form), which
+// centres the stored values on zero and keeps the half-precision mantissa for the deviation from
+// the rest state.
+template <class S>
+struct Store;
+
+template <>
+struct Store<double> {
+  using R = double;
+  static __device__ __forceinline__ double ld(const double* p, int) { return __ldg(p); }
+  static __device__ __forceinline__ double ld_cg(const double* p, int) { return __ldcg(p); }
+  static __device__ __forceinline__ void st(double* p, int, double v) { *p = v; }
+};
+
+template <>
+struct Store<float> {
+  using R = float;
+  static __device__ __forceinline__ float ld(const float* p, int) { return __ldg(p); }
+  static __device__ __forceinline__ float ld_cg(const float* p, int) { return __ldcg(p); }
+  static __device__ __forceinline__ void st(float* p, int, float v) { *p = v; }
+};
+
+template <>
+struct Store<__half> {
+  using R = float;
+  static __device__ __forceinline__ float ld(const __half* p, int i) {
+    return wgt<float>(i) + __half2float(__ldg(p));
+  }
+  static __device__ __forceinline__ float ld_cg(const __half* p, int i) {
+    return wgt<float>(i) + __half2float(__ldcg(p));
+  }
+  static __device__ __forceinline__ void st(__half* p, int i, float v) { *p = __float2half_rn(v - wgt<float>(i)); }
+};
+
+// ------------------------------------------------------------------ helpers
+template <class R>
+__device__ __forceinline__ void set_dir(R* f, int i, R v) {
+#pragma unroll
+  for (int d = 0; d < 9; ++d)
+    if (d == i) f[d] = v;
+}
+
+__device__ __forceinline__ void add_group(double* acc, int g, double vx, double vy) {
+#pragma unroll
+  for (int k = 0; k < kMaxGroups; ++k)
+    if (k == g) { acc[2 * k] += vx; acc[2 * k + 1] += vy; }
+}
+
+// Per-step controls: in channel mode the inlet ramp and the body kick come from the uploaded
+// schedule and the outlet target follows the ramp (src/cases/channel.rs:118-130).
+struct Controls {
+  double vs[4];
+  double target;
+  int has_target;
+};
+
+__device__ __forceinline__ Controls read_controls(const Ctl* c) {
+  Controls k;
+  const unsigned long long t = c->t;
+#pragma unroll
+  for (int g = 0; g < 4; ++g) k.vs[g] = c->vscale[g];
+  k.target = c->target;
+  k.has_target = c->has_target;
+  if (c->sched_on) {
+    const double v1 = t < c->sched_len ? c->sched[2 * t] : 1.0;
+    const double v2 = t < c->sched_len ? c->sched[2 * t + 1] : 0.0;
+    k.vs[1] = v1;
+    k.vs[2] = v2;
+    k.has_target = c->absorbing;
+    k.target = c->u_ref * v1;
+  }
+  return k;
+}
+
+// ------------------------------------------------------------------ epilogue
+// Runs in the last block of a step. `b` is the state after the step.
+template <class S>
+__device__ void step_epilogue(const StepParams& p, const S* __restrict__ b) {
+  using R = typename Store<S>::R;
+  __shared__ double red[kBlock];
+  __shared__ double res[2 * kMaxGroups];
+  __shared__ double rho_c[kProbeCorners];
+  const int tid = threadIdx.x;
+  Ctl* c = p.ctl;
+  const int ncomp = 2 * p.ngroups;
+  // 1) force: each component summed over the link-block partials with a fixed stride pattern,
+  //    then a fixed shared-memory tree (one component at a time, to keep shared memory small).
+  for (int k = 0; k < ncomp; ++k) {
+    double acc = 0.0;
+    for (int blk = tid; blk < p.nlink; blk += kBlock)
+      acc += __ldcg(p.partials + (size_t)blk * (2 * kMaxGroups) + k);
+    red[tid] = acc;
+    __syncthreads();
+    for (int s = kBlock / 2; s > 0; s >>= 1) {
+      if (tid < s) red[tid] += red[tid + s];
+      __syncthreads();
+    }
+    if (tid == 0) res[k] = red[0];
+    __syncthreads();
+  }
+  // 2) pressure-drop probe densities on the new state.
+  if (c->dp_on && tid < kProbeCorners) {
+    const int idx = c->probe_idx[tid];
+    double r = 0.0;
+    if (idx >= 0) {
+      R f[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) f[i] = Store<S>::ld_cg(b + (size_t)i * p.ns + idx, i);
+      double fd[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) fd[i] = (double)f[i];
+      double rr, jx, jy;
+      moments(fd, rr, jx, jy);
+      r = rr;
+    }
+    rho_c[tid] = r;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    const unsigned long long t = c->t;
+    bool finite = true;
+    for (int k = 0; k < 2 * kMaxGroups; ++k) {
+      const double v = k < ncomp ? res[k] : 0.0;
+      c->force[k] = v;
+      if (!isfinite(v)) finite = false;
+    }
+    if (!finite && !c->nonfinite) {
+      c->nonfinite = 1;
+      c->nonfinite_t = t;
+    }
+    double dp = 0.0;
+    if (c->dp_on) {
+      // probe_density (src/sim.rs:624-644) at distances 1, 2, 3 on each side, extrapolated
+      // (src/sim.rs:648-651); pressure drop of src/cases/cylinder.rs:272-277.
+      double wall[2];
+      for (int side = 0; side < 2; ++side) {
+        double pd[3];
+        for (int d = 0; d < 3; ++d) {
+          double sum = 0.0, wsum = 0.0;
+          for (int k = 0; k < 4; ++k) {
+            const int s = (side * 3 + d) * 4 + k;
+            if (c->probe_idx[s] < 0) continue;
+            sum += c->probe_w[s] * rho_c[s];
+            wsum += c->probe_w[s];
+          }
+          pd[d] = wsum > 0.0 ? sum / wsum : __longlong_as_double(0x7ff8000000000000ll);
+        }
+        wall[side] = 3.0 * pd[0] - 3.0 * pd[1] + pd[2];
+      }
+      dp = (1.0 / 3.0) * (wall[0] - wall[1]) / (c->u_ref * c->u_ref);
+    }
+    if (c->rec_cap && t >= c->rec_start && t - c->rec_start < c->rec_cap) {
+      double* r = c->hist + (size_t)(t - c->rec_start) * kRec;
+      for (int k = 0; k < 2 * kMaxGroups; ++k) r[k] = c->force[k];
+      r[8] = c->drho;
+      r[9] = dp;
+    }
+    if (c->sched_on) {
+      const Controls k = read_controls(c);
+      c->vscale[1] = k.vs[1];
+      c->vscale[2] = k.vs[2];
+      c->target = k.target;
+      c->has_target = k.has_target;
+    }
+    c->t = t + 1;
+    c->arrive = 0;
+    __threadfence();
+  }
+}
+
+template <class S>
+__device__ __forceinline__ void arrive(const StepParams& p, const S* __restrict__ b) {
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned prev = atomicAdd(&p.ctl->arrive, 1u);
+    last = prev == (unsigned)(p.nbulk + p.nlink - 1);
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    step_epilogue<S>(p, b);
+  }
+}
+
+// ------------------------------------------------------------------ bulk kernel
+template <class S, int CK>
+__global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepParams p,
+                                                 const S* __restrict__ a, S* __restrict__ b) {
+  using R = typename Store<S>::R;
+  const int nx = p.nx, ny = p.ny;
+  const unsigned ns = p.ns;
+  const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
+  for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
+    const int y = tile / p.tiles_per_row;
+    const int x = (tile - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
+    if (x >= nx) continue;
+    const unsigned idx = (unsigned)(y * nx + x);
+    if (__ldg(p.flag + idx) != 0) continue;
+    const int ym = y == 0 ? ny - 1 : y - 1;
+    const int yp = y == ny - 1 ? 0 : y + 1;
+    const int xm = x == 0 ? nx - 1 : x - 1;
+    const int xp = x == nx - 1 ? 0 : x + 1;
+    const unsigned rc = (unsigned)(y * nx), rm = (unsigned)(ym * nx), rp = (unsigned)(yp * nx);
+    R f[9];
+    f[0] = Store<S>::ld(a + rc + x, 0);
+    f[1] = Store<S>::ld(a + 1u * ns + rc + xm, 1);
+    f[2] = Store<S>::ld(a + 2u * ns + rm + x, 2);
+    f[3] = Store<S>::ld(a + 3u * ns + rc + xp, 3);
+    f[4] = Store<S>::ld(a + 4u * ns + rp + x, 4);
+    f[5] = Store<S>::ld(a + 5u * ns + rm + xm, 5);
+    f[6] = Store<S>::ld(a + 6u * ns + rm + xp, 6);
+    f[7] = Store<S>::ld(a + 7u * ns + rp + xp, 7);
+    f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
+    if (CK == 2)
+      collide_forced(f, op, om, gx, gy);
+    else if (CK == 0)
+      collide_bgk(f, op);
+    else
+      collide_trt(f, op, om);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * ns + idx, i, f[i]);
+  }
+  arrive<S>(p, b);
+}
+
+// ------------------------------------------------------------------ link kernel
+template <class S, int CK>
+__global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepParams p,
+                                                  const S* __restrict__ a, S* __restrict__ b) {
+  using R = typename Store<S>::R;
+  __shared__ double s_un[kBlock];
+  __shared__ double s_drho;
+  __shared__ double s_red[2 * kMaxGroups][kBlock / 32];
+  const int tid = threadIdx.x;
+  const int nx = p.nx, ny = p.ny;
+  const unsigned ns = p.ns;
+  const Controls ctl = read_controls(p.ctl);
+  const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
+
+  // Outlet density offset (src/sim.rs:444-455): velocity of every non-radiating pressure node
+  // from its own populations in `a`, summed sequentially in pnode order.
+  double drho = 0.0;
+  if (ctl.has_target && p.np > 0) {
+    double sum = 0.0;
+    for (int base = 0; base < p.np; base += kBlock) {
+      const int k = base + tid;
+      if (k < p.np) {
+        const int idx = __ldg(p.pnode_idx + k);
+        double f[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+        double rho, jx, jy;
+        moments(f, rho, jx, jy);
+        const double ux = jx / rho - 0.5 * p.gx, uy = jy / rho - 0.5 * p.gy;
+        s_un[tid] = (double)p.pnode_n[2 * k] * ux + (double)p.pnode_n[2 * k + 1] * uy;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        const int m = min(kBlock, p.np - base);
+        for (int q = 0; q < m; ++q) sum += s_un[q];
+      }
+      __syncthreads();
+    }
+    if (tid == 0) s_drho = (sum / (double)p.np - ctl.target) / p.sqrt_cs2;
+    __syncthreads();
+    drho = s_drho;
+  }
+  if (blockIdx.x == 0 && tid == 0) p.ctl->drho = drho;
+
+  double acc[2 * kMaxGroups];
+#pragma unroll
+  for (int k = 0; k < 2 * kMaxGroups; ++k) acc[k] = 0.0;
+
+  const LinkRecDev* links = (const LinkRecDev*)p.links;
+  for (int k = blockIdx.x * kBlock + tid; k < p.nb; k += p.nlink * kBlock) {
+    const int idx = __ldg(p.bnode_idx + k);
+    const int first = __ldg(p.bnode_first + k), last = __ldg(p.bnode_first + k + 1);
+    const int y = idx / nx, x = idx - y * nx;
+    const int ym = y == 0 ? ny - 1 : y - 1;
+    const int yp = y == ny - 1 ? 0 : y + 1;
+    const int xm = x == 0 ? nx - 1 : x - 1;
+    const int xp = x == nx - 1 ? 0 : x + 1;
+    const unsigned rc = (unsigned)(y * nx), rm = (unsigned)(ym * nx), rp = (unsigned)(yp * nx);
+    R f[9];
+    f[0] = Store<S>::ld(a + rc + x, 0);
+    f[1] = Store<S>::ld(a + 1u * ns + rc + xm, 1);
+    f[2] = Store<S>::ld(a + 2u * ns + rm + x, 2);
+    f[3] = Store<S>::ld(a + 3u * ns + rc + xp, 3);
+    f[4] = Store<S>::ld(a + 4u * ns + rp + x, 4);
+    f[5] = Store<S>::ld(a + 5u * ns + rm + xm, 5);
+    f[6] = Store<S>::ld(a + 6u * ns + rm + xp, 6);
+    f[7] = Store<S>::ld(a + 7u * ns + rp + xp, 7);
+    f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
+    bool have_u = false;
+    R ux = R(0), uy = R(0);
+    for (int l = first; l < last; ++l) {
+      const LinkRecDev L = links[l];
+      const int j = L.dir;
+      const int i = opp_of(j);
+      const R out = Store<S>::ld(a + (unsigned)j * ns + idx, j);
+      const R scale = (R)ctl.vs[L.vgroup];
+      R back;
+      if (!(L.flags & 1)) {
+        // Wall: interpolated bounce-back with the moving-wall term (src/sim.rs:467-479).
+        const R corr = (R)L.cu6 * scale;
+        const R q = (R)L.q;
+        if (q >= R(0.5)) {
+          const R kq = R(0.5) / q;
+          back = kq * (out - corr) + (R(1.0) - kq) * Store<S>::ld(a + (unsigned)i * ns + idx, i);
+        } else if (L.behind >= 0) {
+          back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * Store<S>::ld(a + (unsigned)j * ns + (unsigned)L.behind, j) - corr;
+        } else {
+          back = out - corr;
+        }
+      } else {
+        // Open boundary: anti-bounce-back around the equilibrium of the boundary density
+        // (src/sim.rs:480-488), with the node's own velocity.
+        if (!have_u) {
+          R g[9];
+#pragma unroll
+          for (int d = 0; d < 9; ++d) g[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
+          R rho, jx, jy;
+          moments(g, rho, jx, jy);
+          ux = jx / rho - R(0.5) * gx;
+          uy = jy / rho - R(0.5) * gy;
+          have_u = true;
+        }
+        const R cu = R(3.0) * ((R)cx_of(j) * ux + (R)cy_of(j) * uy);
+        R rho_w;
+        if (L.flags & 2) {
+          const R nxv = (R)((int)((L.flags >> 2) & 3) - 1), nyv = (R)((int)((L.flags >> 4) & 3) - 1);
+          rho_w = (R)L.rho + (nxv * ux + nyv * uy) / (R)p.sqrt_cs2;
+        } else {
+          rho_w = (R)L.rho + (R)drho;
+        }
+        back = -out + R(2.0) * (R)w_of(j) * rho_w * (R(1.0) + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy));
+      }
+      set_dir(f, i, back);
+      if (L.fgroup >= 0) {
+        // Galilean-invariant momentum exchange (src/sim.rs:490-495), accumulated in FP64.
+        const double o = (double)out, bk = (double)back;
+        const double wux = L.uw0 * (double)scale, wuy = L.uw1 * (double)scale;
+        const double fxc = (double)cx_of(j) * (o + bk) - wux * (o - bk);
+        const double fyc = (double)cy_of(j) * (o + bk) - wuy * (o - bk);
+        add_group(acc, L.fgroup, fxc, fyc);
+      }
+    }
+    if (CK == 2)
+      collide_forced(f, op, om, gx, gy);
+    else if (CK == 0)
+      collide_bgk(f, op);
+    else
+      collide_trt(f, op, om);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * ns + idx, i, f[i]);
+  }
+
+  // Block partial of the force: fixed shuffle tree within each warp, then fixed order over warps.
+  if (p.ngroups > 0) {
+    const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+    for (int k = 0; k < 2 * kMaxGroups; ++k) {
+      double v = acc[k];
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) s_red[k][warp] = v;
+    }
+    __syncthreads();
+    if (tid < 2 * kMaxGroups) {
+      double v = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) v += s_red[tid][w];
+      p.partials[(size_t)blockIdx.x * (2 * kMaxGroups) + tid] = v;
+    }
+  }
+  arrive<S>(p, b);
+}
+
+// ------------------------------------------------------------------ utility kernels
+// Sim::init (src/sim.rs:357-371): equilibrium of a field into both buffers; solids get (1,0,0).
+template <class S>
+__global__ void k_init(int n, unsigned ns, const uint8_t* __restrict__ flag, const double* __restrict__ rho,
+                       const double* __restrict__ ux, const double* __restrict__ uy, double rho0, double ux0,
+                       double uy0, S* __restrict__ a, S* __restrict__ b) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    double r = rho0, u = ux0, v = uy0;
+    if (flag[idx] == 2) {
+      r = 1.0; u = 0.0; v = 0.0;
+    } else if (rho) {
+      r = rho[idx]; u = ux[idx]; v = uy[idx];
+    }
+    double feq[9];
+    equilibrium(r, u, v, feq);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      Store<S>::st(a + (size_t)i * ns + idx, i, (typename Store<S>::R)feq[i]);
+      Store<S>::st(b + (size_t)i * ns + idx, i, (typename Store<S>::R)feq[i]);
+    }
+  }
+}
+
+// Populations to FP64 in the reference layout (plane stride n).
+template <class S>
+__global__ void k_to_f64(int n, unsigned ns, const S* __restrict__ a, double* __restrict__ out) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) out[(size_t)i * n + idx] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+  }
+}
+
+// FP64 populations (reference layout) into storage S.
+template <class S>
+__global__ void k_from_f64(int n, unsigned ns, const double* __restrict__ in, S* __restrict__ a) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i)
+      Store<S>::st(a + (size_t)i * ns + idx, i, (typename Store<S>::R)in[(size_t)i * n + idx]);
+  }
+}
+
+// (rho, ux, uy) of every cell as Sim::macros computes them (src/sim.rs:527-534); solids (1,0,0).
+template <class S>
+__global__ void k_macros(int n, unsigned ns, const uint8_t* __restrict__ flag, double gx, double gy,
+                         const S* __restrict__ a, double* __restrict__ rho, double* __restrict__ ux,
+                         double* __restrict__ uy) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    if (flag[idx] == 2) {
+      rho[idx] = 1.0; ux[idx] = 0.0; uy[idx] = 0.0;
+      continue;
+    }
+    double f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+    double r, jx, jy;
+    moments(f, r, jx, jy);
+    rho[idx] = r;
+    ux[idx] = jx / r - 0.5 * gx;
+    uy[idx] = jy / r - 0.5 * gy;
+  }
+}
+
+// Deterministic FP64 reductions over fluid cells: per-thread Neumaier sums of mass and the two
+// momentum components (src/sim.rs:538-563), then a fixed pairwise tree; plus the largest speed
+// with NaN propagation (src/sim.rs:566-579). One block per slot of `out` (4 doubles per block).
+__device__ __forceinline__ void neumaier_add(double& s, double& c, double x) {
+  const double t = s + x;
+  c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_reduce(int n, unsigned ns, const uint8_t* __restrict__ flag,
+                                                   double gx, double gy, const S* __restrict__ a,
+                                                   double* __restrict__ out) {
+  __shared__ double sh[7][kBlock];
+  double ms = 0, mc = 0, xs = 0, xc = 0, ys = 0, yc = 0, vmax = 0.0;
+  bool nan = false;
+  for (int idx = blockIdx.x * kBlock + threadIdx.x; idx < n; idx += gridDim.x * kBlock) {
+    if (flag[idx] == 2) continue;
+    double f[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) neumaier_add(ms, mc, f[i]);
+#pragma unroll
+    for (int i = 1; i < 9; ++i) {
+      neumaier_add(xs, xc, (double)cx_of(i) * f[i]);
+      neumaier_add(ys, yc, (double)cy_of(i) * f[i]);
+    }
+    double r, jx, jy;
+    moments(f, r, jx, jy);
+    const double u = jx / r - 0.5 * gx, v = jy / r - 0.5 * gy;
+    const double sp = sqrt(u * u + v * v);
+    if (isnan(sp)) nan = true; else vmax = fmax(vmax, sp);
+  }
+  const int t = threadIdx.x;
+  sh[0][t] = ms; sh[1][t] = mc; sh[2][t] = xs; sh[3][t] = xc; sh[4][t] = ys; sh[5][t] = yc;
+  sh[6][t] = nan ? __longlong_as_double(0x7ff8000000000000ll) : vmax;
+  __syncthreads();
+  for (int s = kBlock / 2; s > 0; s >>= 1) {
+    if (t < s) {
+      for (int k = 0; k < 3; ++k) {
+        double s0 = sh[2 * k][t], c0 = sh[2 * k + 1][t];
+        neumaier_add(s0, c0, sh[2 * k][t + s]);
+        sh[2 * k][t] = s0;
+        sh[2 * k + 1][t] = c0 + sh[2 * k + 1][t + s];
+      }
+      const double o = sh[6][t + s], m = sh[6][t];
+      sh[6][t] = (isnan(o) || isnan(m)) ? __longlong_as_double(0x7ff8000000000000ll) : fmax(m, o);
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    double* o = out + 7 * blockIdx.x;
+    for (int k = 0; k < 7; ++k) o[k] = sh[k][0];
+  }
+}
+
+// Gathers the 9 populations (as FP64) of a list of cells.
+template <class S>
+__global__ void k_gather(int m, unsigned ns, const int32_t* __restrict__ cells, const S* __restrict__ a,
+                         double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const int idx = cells[k];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) out[9 * k + i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+}
+
+}  // namespace vl

@@ -1,0 +1,35 @@
+// Host-side table of kernel launchers, one per population storage precision. The FP64 table is
+// compiled without FMA contraction (bit-identical to the reference); the FP32 and FP16-shifted
+// tables are compiled with it.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+namespace vl {
+
+struct StepParams;
+
+struct Launchers {
+  size_t elem;  // bytes per stored population value
+  // One step: the link kernel then the bulk kernel, both on `s`. ck: 0 BGK, 1 TRT, 2 forced.
+  cudaError_t (*step)(const StepParams& p, int ck, const void* a, void* b, cudaStream_t s);
+  cudaError_t (*init)(int n, unsigned ns, const uint8_t* flag, const double* rho, const double* ux,
+                      const double* uy, double rho0, double ux0, double uy0, void* a, void* b, cudaStream_t s);
+  cudaError_t (*to_f64)(int n, unsigned ns, const void* a, double* out, cudaStream_t s);
+  cudaError_t (*from_f64)(int n, unsigned ns, const double* in, void* a, cudaStream_t s);
+  cudaError_t (*macros)(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,
+                        double* rho, double* ux, double* uy, cudaStream_t s);
+  cudaError_t (*reduce)(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,
+                        double* out, int blocks, cudaStream_t s);
+  cudaError_t (*gather)(int m, unsigned ns, const int32_t* cells, const void* a, double* out, cudaStream_t s);
+  // Resident blocks per SM of the bulk kernel (for grid sizing).
+  int (*bulk_occupancy)(int ck);
+};
+
+const Launchers& launchers_f64();
+const Launchers& launchers_f32();
+const Launchers& launchers_f16s();
+
+}  // namespace vl

@@ -1,0 +1,76 @@
+// Launcher bodies shared by the per-precision translation units.
+#pragma once
+
+#include "vl_device.cuh"
+#include "vl_launch.hpp"
+
+namespace vl {
+
+template <class S>
+struct LaunchImpl {
+  // which: 3 = both kernels of the step, 1 = the link kernel only, 2 = the bulk kernel only
+  // (a step launched in two halves, for per-kernel timing).
+  template <int CK>
+  static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which) {
+    if ((which & 1) && p.nlink > 0) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
+    if (which & 2) k_bulk<S, CK><<<p.nbulk, kBlock, 0, s>>>(p, a, b);
+    return cudaGetLastError();
+  }
+  // ck: collision kind (0 BGK, 1 TRT, 2 forced) in the low byte; bit 8 = link kernel only,
+  // bit 9 = bulk kernel only.
+  static cudaError_t step(const StepParams& p, int ck, const void* a, void* b, cudaStream_t s) {
+    const S* A = (const S*)a;
+    S* B = (S*)b;
+    const int which = (ck & 0x300) ? ((ck & 0x100) ? 1 : 0) | ((ck & 0x200) ? 2 : 0) : 3;
+    switch (ck & 0xff) {
+      case 0: return step_ck<0>(p, A, B, s, which);
+      case 2: return step_ck<2>(p, A, B, s, which);
+      default: return step_ck<1>(p, A, B, s, which);
+    }
+  }
+  static int grid_for(int n) { return n <= 0 ? 1 : (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16; }
+  static cudaError_t init(int n, unsigned ns, const uint8_t* flag, const double* rho, const double* ux,
+                          const double* uy, double rho0, double ux0, double uy0, void* a, void* b, cudaStream_t s) {
+    k_init<S><<<grid_for(n), 256, 0, s>>>(n, ns, flag, rho, ux, uy, rho0, ux0, uy0, (S*)a, (S*)b);
+    return cudaGetLastError();
+  }
+  static cudaError_t to_f64(int n, unsigned ns, const void* a, double* out, cudaStream_t s) {
+    k_to_f64<S><<<grid_for(n), 256, 0, s>>>(n, ns, (const S*)a, out);
+    return cudaGetLastError();
+  }
+  static cudaError_t from_f64(int n, unsigned ns, const double* in, void* a, cudaStream_t s) {
+    k_from_f64<S><<<grid_for(n), 256, 0, s>>>(n, ns, in, (S*)a);
+    return cudaGetLastError();
+  }
+  static cudaError_t macros(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,
+                            double* rho, double* ux, double* uy, cudaStream_t s) {
+    k_macros<S><<<grid_for(n), 256, 0, s>>>(n, ns, flag, gx, gy, (const S*)a, rho, ux, uy);
+    return cudaGetLastError();
+  }
+  static cudaError_t reduce(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,
+                            double* out, int blocks, cudaStream_t s) {
+    k_reduce<S><<<blocks, kBlock, 0, s>>>(n, ns, flag, gx, gy, (const S*)a, out);
+    return cudaGetLastError();
+  }
+  static cudaError_t gather(int m, unsigned ns, const int32_t* cells, const void* a, double* out, cudaStream_t s) {
+    if (m <= 0) return cudaSuccess;
+    k_gather<S><<<(m + 127) / 128, 128, 0, s>>>(m, ns, cells, (const S*)a, out);
+    return cudaGetLastError();
+  }
+  static int bulk_occupancy(int ck) {
+    int blocks = 0;
+    cudaError_t e;
+    switch (ck) {
+      case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 0>, kBlock, 0); break;
+      case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 2>, kBlock, 0); break;
+      default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 1>, kBlock, 0); break;
+    }
+    return (e == cudaSuccess && blocks > 0) ? blocks : 1;
+  }
+  static const Launchers& table() {
+    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &bulk_occupancy};
+    return t;
+  }
+};
+
+}  // namespace vl

@@ -1,0 +1,8 @@
+// Reduced-precision step kernels: FP32 storage and FP16 storage of f_i - w_i, both with FP32
+// collision arithmetic; the force accumulation and every reduction stay in FP64.
+#include "vl_launch_impl.cuh"
+
+namespace vl {
+const Launchers& launchers_f32() { return LaunchImpl<float>::table(); }
+const Launchers& launchers_f16s() { return LaunchImpl<__half>::table(); }
+}  // namespace vl
