@@ -177,7 +177,7 @@ def channel_n80(V):
     ch, secs = V.cylinder.bench(V.cylinder.Setup(n=80), 1000)
     h = ch.sim.state_hash()
     out = {"grid": f"{ch.sim.nx}x{ch.sim.ny}", "fluid_nodes": ch.sim.fluid_nodes(), "steps": 1000,
-           "mlups": round(ch.sim.fluid_nodes() * 1000 / secs / 1e6, 1), "ms_per_step": round(secs, 6),
+           "mlups": round(ch.sim.fluid_nodes() * 1000 / secs / 1e6, 1), "ms_per_step": round(secs * 1e3 / 1000, 5),
            "state_hash": f"{h:016x}", "published_hash_match": f"{h:016x}" == "c93e26bfa33474ee"}
     ch.close()
     return out
@@ -203,6 +203,9 @@ def run_vortexlab(args):
     interior = int(np.count_nonzero(flags == 0))
     fluid = sim.fluid_nodes()
     sim.init((1.0, BOX["u"], 0.0))
+    tune = sim.autotune(8) if args.schedule == "auto" else None
+    if args.schedule != "auto":
+        sim.schedule = args.schedule
     sim.step(max(args.warmup, 3))
     sim.synchronize()
     if dist:
@@ -268,7 +271,8 @@ def run_vortexlab(args):
         "config": {"workload": workload_name(prec), "grid": [nx, ny], "fluid_nodes": fluid, "interior_nodes": interior,
                    "links": sim.link_count(), "boundary_nodes": sim.bnode_count(), "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (populations 2 x 9 x 33.5M values), no flush needed",
-                   "timing": "CUDA events around every kernel on the sim's stream, max over ranks",
+                   "timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
+                   "schedule": sim.schedule, "autotune_ms_per_step": tune,
                    "setup_s": round(setup_s, 2)},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
@@ -304,7 +308,12 @@ def main():
     ap.add_argument("--precision", choices=["f64", "f32", "f16s"], default="f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first"])
+    ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
     args = ap.parse_args()
+    if args.box:
+        nx, ny = (int(v) for v in args.box.lower().split("x"))
+        BOX.update(nx=nx, ny=ny)
     if args.impl == "reference":
         return run_reference(args)
     return run_vortexlab(args)

@@ -157,3 +157,25 @@ def test_graph_and_single_steps_agree(gpu):
                 r.ch.step(1)
         hashes.append((r.ch.sim.state_hash(), r.ch.sim.force.tobytes()))
     assert hashes[0] == hashes[1]
+
+
+def test_schedules_and_autotune_do_not_change_results(gpu):
+    """The three kernel orders give bit-identical states; autotuning (dry-run timing) leaves t,
+    the force, the history and the state untouched."""
+    V = gpu
+    results = []
+    for sched in ("concurrent", "links-first", "bulk-first", "auto"):
+        r = V.cylinder.rig(V.cylinder.Setup(n=10), 100.0, 1.0)
+        sim = r.ch.sim
+        sim.record(300)
+        r.ch.step(150)
+        if sched == "auto":
+            t0, f0 = sim.t, sim.force.copy()
+            ms = sim.autotune(4)
+            assert set(ms) == {"concurrent", "links-first", "bulk-first"}
+            assert sim.t == t0 and np.array_equal(sim.force, f0)
+        else:
+            sim.schedule = sched
+        r.ch.step(150)
+        results.append((sim.state_hash(), sim.history().tobytes()))
+    assert all(x == results[0] for x in results)

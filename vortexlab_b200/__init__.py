@@ -632,6 +632,24 @@ class Sim:
         check(lib.vl_sim_step_profiled(self._h, n, C.byref(lk), C.byref(bk), C.byref(tot)))
         return lk.value, bk.value, tot.value
 
+    SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2}
+
+    @property
+    def schedule(self) -> str:
+        inv = {v: k for k, v in self.SCHEDULES.items()}
+        return inv[check(lib.vl_sim_get_schedule(self._h))]
+
+    @schedule.setter
+    def schedule(self, name: str):
+        check(lib.vl_sim_set_schedule(self._h, self.SCHEDULES[name]))
+
+    def autotune(self, steps_each: int = 8):
+        """Times the three kernel schedules without advancing the state; keeps the fastest.
+        Returns {schedule: ms per step}."""
+        out = np.zeros(3)
+        check(lib.vl_sim_autotune(self._h, steps_each, _dp(out)))
+        return dict(zip(self.SCHEDULES, out.tolist()))
+
     def launch_count(self) -> int:
         out = C.c_uint64()
         check(lib.vl_sim_launch_count(self._h, C.byref(out)))

@@ -36,12 +36,12 @@ def _cxx():
     return os.environ.get("CXX") or shutil.which("g++") or "g++"
 
 
-def _sources():
+def _sources(defines=()):
     cxx, nvcc = _cxx(), _nvcc()
     inc = ["-I", CSRC, "-I", os.path.join(os.path.dirname(HERE), "include")]
     host_flags = ["-O3", "-std=c++17", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-Wall"]
     cu_flags = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
-                       "--expt-relaxed-constexpr", "-Xptxas", "-v"]
+                       "--expt-relaxed-constexpr", "-Xptxas", "-v"] + [f"-D{d}" for d in defines]
     jobs = [
         ("vl_host.o", [cxx] + host_flags + inc + ["-c", os.path.join(CSRC, "vl_host.cpp")]),
         ("vl_api.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_api.cu")]),
@@ -67,11 +67,16 @@ def _deps():
     return out + [os.path.abspath(__file__)]
 
 
-def build(verbose: bool = False, force: bool = False) -> str:
-    """Compiles every translation unit that is out of date and links the shared library."""
+def build(verbose: bool = False, force: bool = False, out: str = LIB, defines=(), build_dir: str = BUILD) -> str:
+    """Compiles every translation unit that is out of date and links the shared library.
+
+    ``defines`` (NAME=VALUE strings) and ``out`` / ``build_dir`` build a variant of the library
+    elsewhere, for example with other launch bounds, without touching the default build."""
+    global BUILD, LIB
+    BUILD, LIB = build_dir, out
     os.makedirs(BUILD, exist_ok=True)
     deps = _deps()
-    jobs = _sources()
+    jobs = _sources(defines)
     todo = [(o, cmd) for o, cmd in jobs if force or _stale(os.path.join(BUILD, o), deps)]
 
     def run(item):
@@ -101,4 +106,11 @@ def build(verbose: bool = False, force: bool = False) -> str:
 
 
 if __name__ == "__main__":
-    build(verbose=True, force="--force" in sys.argv)
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--out", default=LIB)
+    ap.add_argument("--build-dir", default=BUILD)
+    ap.add_argument("-D", dest="defines", action="append", default=[])
+    a = ap.parse_args()
+    build(verbose=True, force=a.force, out=a.out, defines=a.defines, build_dir=a.build_dir)

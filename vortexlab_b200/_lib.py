@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libvortexlab_b200.so")
+# VORTEXLAB_B200_LIB selects another build of the same library (for example a profiling variant).
+LIB_PATH = os.environ.get("VORTEXLAB_B200_LIB") or os.path.join(HERE, "libvortexlab_b200.so")
 
 VL_OK, VL_EINVAL, VL_ECUDA, VL_EDIVERGED, VL_ENOMEM, VL_EUNSUPPORTED = 0, -1, -2, -3, -4, -5
 VL_REC = 10
@@ -109,6 +110,9 @@ def _declare(L):
         "vl_sim_set_dp_probe": (i, [vp, d, d, d, d]),
         "vl_sim_last_step_ms": (i, [vp, P(f)]),
         "vl_sim_step_profiled": (i, [vp, u64, P(d), P(d), P(d)]),
+        "vl_sim_set_schedule": (i, [vp, i]),
+        "vl_sim_get_schedule": (i, [vp]),
+        "vl_sim_autotune": (i, [vp, i, P(d)]),
         "vl_sim_launch_count": (i, [vp, P(u64)]),
         "vl_channel_new": (vp, [P(vl_channel_spec), i]),
         "vl_channel_free": (None, [vp]),

@@ -77,13 +77,18 @@ struct vl_sim {
   double* d_red = nullptr;
   int32_t* d_cells = nullptr;
   double* d_gather = nullptr;
-  cudaStream_t stream = nullptr;
+  cudaStream_t stream = nullptr;   // the sim's stream: bulk kernel, copies, everything else
+  cudaStream_t aux = nullptr;      // the link kernel of each step, forked from and joined to `stream`
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   vl::StepParams P{};
   int ck = 1;
   cudaGraphExec_t gexec = nullptr;
   uint64_t launches = 0;
   int kernels_per_step = 1;
+  // Order of the two kernels of a step: 0 concurrent (fork/join over two streams), 1 link kernel
+  // then bulk kernel on one stream, 2 bulk then link.
+  int schedule = 0;
   uint64_t t_host = 0;
   uint64_t rec_start = 0, rec_cap = 0;
   bool timed = false;
@@ -100,6 +105,9 @@ struct vl_sim {
     for (cudaEvent_t e : pev) cudaEventDestroy(e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
   }
 
@@ -117,8 +125,101 @@ struct vl_sim {
     return VL_OK;
   }
 
+  // One step: the link kernel on `aux` and the bulk kernel on `stream`, concurrently. They read
+  // only `a` and write disjoint cells of `b`; the join makes the next step wait for both. Optional
+  // timing events bracket each kernel on its own stream.
+  cudaError_t enqueue_step(cudaEvent_t lk0 = nullptr, cudaEvent_t lk1 = nullptr, cudaEvent_t bk0 = nullptr,
+                           cudaEvent_t bk1 = nullptr) {
+    cudaError_t e;
+    cudaStream_t ls = schedule == 0 ? aux : stream;
+    auto links = [&]() -> cudaError_t {
+      cudaError_t r;
+      if (lk0 && (r = cudaEventRecord(lk0, ls)) != cudaSuccess) return r;
+      if ((r = L->step(P, ck | 0x100, a(), b(), ls)) != cudaSuccess) return r;
+      if (lk1 && (r = cudaEventRecord(lk1, ls)) != cudaSuccess) return r;
+      return cudaSuccess;
+    };
+    auto bulk = [&]() -> cudaError_t {
+      cudaError_t r;
+      if (bk0 && (r = cudaEventRecord(bk0, stream)) != cudaSuccess) return r;
+      if ((r = L->step(P, ck | 0x200, a(), b(), stream)) != cudaSuccess) return r;
+      if (bk1 && (r = cudaEventRecord(bk1, stream)) != cudaSuccess) return r;
+      return cudaSuccess;
+    };
+    if (schedule == 1) {
+      if ((e = links()) != cudaSuccess) return e;
+      return bulk();
+    }
+    if (schedule == 2) {
+      if ((e = bulk()) != cudaSuccess) return e;
+      return links();
+    }
+    if ((e = cudaEventRecord(ev_fork, stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(aux, ev_fork, 0)) != cudaSuccess) return e;
+    if ((e = links()) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_join, aux)) != cudaSuccess) return e;
+    if ((e = bulk()) != cudaSuccess) return e;
+    return cudaStreamWaitEvent(stream, ev_join, 0);
+  }
+
+  int set_schedule(int sc) {
+    if (sc < 0 || sc > 2) return fail(VL_EINVAL, "schedule must be 0, 1 or 2");
+    if (sc != schedule && gexec) {
+      VL_CUDA(cudaStreamSynchronize(stream));
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    schedule = sc;
+    return VL_OK;
+  }
+
+  // Times every schedule on the current state without advancing it: the control block is put in
+  // dry mode (the epilogue commits nothing) and each timed step recomputes `b` from the same `a`.
+  int autotune(int steps_each, double* ms_out) {
+    VL_CUDA(cudaSetDevice(device));
+    int rc = pull_ctl();
+    if (rc) return rc;
+    hctl.dry = 1;
+    if ((rc = push_ctl())) return rc;
+    double best = 1e300;
+    int best_sc = schedule;
+    for (int sc = 0; sc < 3; ++sc) {
+      schedule = sc;
+      for (int k = 0; k < 2; ++k) {
+        cudaError_t e = enqueue_step();
+        if (e != cudaSuccess) return cuda_fail(e, "autotune");
+      }
+      VL_CUDA(cudaEventRecord(ev0, stream));
+      for (int k = 0; k < steps_each; ++k) {
+        cudaError_t e = enqueue_step();
+        if (e != cudaSuccess) return cuda_fail(e, "autotune");
+      }
+      VL_CUDA(cudaEventRecord(ev1, stream));
+      VL_CUDA(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      VL_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      if (ms_out) ms_out[sc] = ms / steps_each;
+      if (ms < best) { best = ms; best_sc = sc; }
+    }
+    if ((rc = pull_ctl())) return rc;
+    hctl.dry = 0;
+    if ((rc = push_ctl())) return rc;
+    schedule = -1;
+    return set_schedule(best_sc);
+  }
+
+  // The pressure probe of step t is evaluated during step t + 1; the last step of a batch gets
+  // it from this one-block kernel.
+  int flush_probe() {
+    if (!hctl.dp_on) return VL_OK;
+    cudaError_t e = L->probe(P, a(), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "probe launch");
+    launches += 1;
+    return VL_OK;
+  }
+
   int launch_one() {
-    cudaError_t e = L->step(P, ck, a(), b(), stream);
+    cudaError_t e = enqueue_step();
     if (e != cudaSuccess) return cuda_fail(e, "step launch");
     cur ^= 1;
     launches += (uint64_t)kernels_per_step;
@@ -132,7 +233,7 @@ struct vl_sim {
     int saved = cur;
     cur = 0;
     for (int k = 0; k < kGraphSteps; ++k) {
-      cudaError_t e = L->step(P, ck, a(), b(), stream);
+      cudaError_t e = enqueue_step();
       cur ^= 1;
       if (e != cudaSuccess) {
         cudaStreamEndCapture(stream, &g);
@@ -169,7 +270,7 @@ struct vl_sim {
     VL_CUDA(cudaEventRecord(ev1, stream));
     timed = true;
     t_host += steps;
-    return VL_OK;
+    return flush_probe();
   }
 
   // Steps launched one by one with CUDA events around each kernel on the sim's stream; returns
@@ -177,42 +278,38 @@ struct vl_sim {
   std::vector<cudaEvent_t> pev;
   int step_profiled(uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms) {
     VL_CUDA(cudaSetDevice(device));
-    const size_t need = 2 * (size_t)steps + 1;
+    const size_t need = 4 * (size_t)steps + 2;
     while (pev.size() < need) {
       cudaEvent_t e;
       VL_CUDA(cudaEventCreate(&e));
       pev.push_back(e);
     }
-    const bool has_links = P.nlink > 0;
     VL_CUDA(cudaEventRecord(pev[0], stream));
     for (uint64_t k = 0; k < steps; ++k) {
-      // links then bulk, as one step launches them, with an event after each
-      cudaError_t e = cudaSuccess;
-      if (has_links) e = L->step(P, ck | 0x100, a(), b(), stream);
+      cudaEvent_t* e4 = &pev[2 + 4 * k];
+      cudaError_t e = enqueue_step(e4[0], e4[1], e4[2], e4[3]);
       if (e != cudaSuccess) return cuda_fail(e, "profiled step");
-      VL_CUDA(cudaEventRecord(pev[2 * k + 1], stream));
-      e = L->step(P, ck | 0x200, a(), b(), stream);
-      if (e != cudaSuccess) return cuda_fail(e, "profiled step");
-      VL_CUDA(cudaEventRecord(pev[2 * k + 2], stream));
       cur ^= 1;
       launches += (uint64_t)kernels_per_step;
     }
-    VL_CUDA(cudaEventSynchronize(pev[2 * steps]));
+    VL_CUDA(cudaEventRecord(pev[1], stream));
+    VL_CUDA(cudaEventSynchronize(pev[1]));
     double lk = 0.0, bk = 0.0;
     for (uint64_t k = 0; k < steps; ++k) {
-      float m1 = 0.f, m2 = 0.f;
-      VL_CUDA(cudaEventElapsedTime(&m1, pev[2 * k], pev[2 * k + 1]));
-      VL_CUDA(cudaEventElapsedTime(&m2, pev[2 * k + 1], pev[2 * k + 2]));
-      lk += m1;
-      bk += m2;
+      const cudaEvent_t* e4 = &pev[2 + 4 * k];
+      float m = 0.f;
+      VL_CUDA(cudaEventElapsedTime(&m, e4[0], e4[1]));
+      lk += m;
+      VL_CUDA(cudaEventElapsedTime(&m, e4[2], e4[3]));
+      bk += m;
     }
     float tot = 0.f;
-    VL_CUDA(cudaEventElapsedTime(&tot, pev[0], pev[2 * steps]));
+    VL_CUDA(cudaEventElapsedTime(&tot, pev[0], pev[1]));
     if (link_ms) *link_ms = lk;
     if (bulk_ms) *bulk_ms = bk;
     if (total_ms) *total_ms = tot;
     t_host += steps;
-    return VL_OK;
+    return flush_probe();
   }
 
   // 9 FP64 populations of each listed cell (reference order).
@@ -340,14 +437,15 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
       !chk(alloc_copy((void**)&s->d_gather, nullptr, 64 * 9 * sizeof(double))))
     return nullptr;
   if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&s->aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreate(&s->ev0) != cudaSuccess || cudaEventCreate(&s->ev1) != cudaSuccess) {
     fail(VL_ECUDA, "stream/event creation");
     return nullptr;
   }
-  // Launch geometry: the bulk kernel sized to one full wave of resident blocks (grid-stride over
-  // row tiles); the link kernel to at most two blocks per SM.
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->device);
+  // Launch geometry: one bulk block per row tile of kBlock cells; one link thread per boundary
+  // node, and at least one link block (it runs the end-of-step epilogue).
   const bool forced = d.accel[0] != 0.0 || d.accel[1] != 0.0;
   s->ck = forced ? 2 : (d.collision == vl::COLL_BGK ? 0 : 1);
   vl::StepParams& P = s->P;
@@ -356,11 +454,10 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.ns = s->ns;
   P.tiles_per_row = (int)((d.nx + vl::kBlock - 1) / vl::kBlock);
   P.ntiles = P.tiles_per_row * (int)d.ny;
-  const int occ = s->L->bulk_occupancy(s->ck);
-  P.nbulk = std::max(1, std::min(P.ntiles, sms * occ));
+  P.nbulk = P.ntiles;
   const int nb = (int)d.bnode_idx.size();
-  P.nlink = nb == 0 ? 0 : std::max(1, std::min((nb + vl::kBlock - 1) / vl::kBlock, 2 * sms));
-  s->kernels_per_step = P.nlink > 0 ? 2 : 1;
+  P.nlink = std::max(1, (nb + vl::kBlock - 1) / vl::kBlock);
+  s->kernels_per_step = 2;
   P.coll = d.collision;
   P.forced = forced ? 1 : 0;
   P.op = d.op;
@@ -378,7 +475,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.np = (int)d.pnode_idx.size();
   P.ctl = s->d_ctl;
   P.ngroups = d.ngroups;
-  if (!chk(alloc_copy((void**)&s->d_partials, nullptr, (size_t)std::max(P.nlink, 1) * 2 * vl::kMaxGroups * sizeof(double))))
+  if (!chk(alloc_copy((void**)&s->d_partials, nullptr, (size_t)P.nlink * 2 * vl::kMaxGroups * sizeof(double))))
     return nullptr;
   P.partials = s->d_partials;
   // Control block: vscale = 1, no outflow target (src/sim.rs:344-347).
@@ -997,6 +1094,18 @@ int vl_sim_last_step_ms(vl_sim* s, float* ms) {
   VL_CUDA(cudaEventSynchronize(s->ev1));
   VL_CUDA(cudaEventElapsedTime(ms, s->ev0, s->ev1));
   return VL_OK;
+}
+
+int vl_sim_set_schedule(vl_sim* s, int schedule) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  return s->set_schedule(schedule);
+}
+
+int vl_sim_get_schedule(const vl_sim* s) { return s ? s->schedule : VL_EINVAL; }
+
+int vl_sim_autotune(vl_sim* s, int steps_each, double* ms3) {
+  if (!s || steps_each < 1) return fail(VL_EINVAL, "autotune: bad arguments");
+  return s->autotune(steps_each, ms3);
 }
 
 int vl_sim_step_profiled(vl_sim* s, uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms) {

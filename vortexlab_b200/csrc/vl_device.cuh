@@ -1,11 +1,12 @@
 // Device data structures and the step kernels (templated on storage and arithmetic type).
 //
-// One time step of the reference (src/sim.rs:391-420) is two kernels on one stream:
+// One time step of the reference (src/sim.rs:391-420) is two kernels that run concurrently
+// (a fork/join over two streams, captured into the step graph):
 //
 //   k_links  boundary nodes: gather the 9 incoming populations, replace every population that
 //            would come out of a wall or open boundary with the boundary rule of its link
 //            (src/sim.rs:456-507), accumulate the momentum-exchange force per force group,
-//            collide, write. One thread per boundary node, grid-stride over the CSR node list.
+//            collide, write. One thread per boundary node of the CSR node list.
 //   k_bulk   interior nodes (flag 0): pull the 9 populations from the upstream neighbours with
 //            periodic wrap (src/sim.rs:700-735), collide, write. One thread per cell of a
 //            row tile, grid-stride over tiles.
@@ -48,6 +49,7 @@ struct Ctl {
   int has_target;
   int nonfinite;               // set once a non-finite force is seen
   int sched_on;                // channel mode: controls from the schedule below
+  int dry;                     // timing runs: the epilogue commits nothing (no t, force or history)
   int absorbing;
   int dp_on;
   double u_ref;
@@ -125,16 +127,19 @@ struct Store<__half> {
 
 // ------------------------------------------------------------------ helpers
 template <class R>
+__device__ __forceinline__ R pick(const R* f, int i) {
+  R v = f[0];
+#pragma unroll
+  for (int d = 1; d < 9; ++d)
+    if (d == i) v = f[d];
+  return v;
+}
+
+template <class R>
 __device__ __forceinline__ void set_dir(R* f, int i, R v) {
 #pragma unroll
   for (int d = 0; d < 9; ++d)
     if (d == i) f[d] = v;
-}
-
-__device__ __forceinline__ void add_group(double* acc, int g, double vx, double vy) {
-#pragma unroll
-  for (int k = 0; k < kMaxGroups; ++k)
-    if (k == g) { acc[2 * k] += vx; acc[2 * k + 1] += vy; }
 }
 
 // Per-step controls: in channel mode the inlet ramp and the body kick come from the uploaded
@@ -164,18 +169,62 @@ __device__ __forceinline__ Controls read_controls(const Ctl* c) {
 }
 
 // ------------------------------------------------------------------ epilogue
-// Runs in the last block of a step. `b` is the state after the step.
+// Pressure-drop probe (src/cases/cylinder.rs:272-277) of the state `a` recorded as step `tstep`
+// of the history: probe_density (src/sim.rs:624-644) at distances 1, 2, 3 from each wall point,
+// extrapolated to the wall (src/sim.rs:648-651). Block-wide; every thread must call it.
 template <class S>
-__device__ void step_epilogue(const StepParams& p, const S* __restrict__ b) {
-  using R = typename Store<S>::R;
+__device__ void record_probe(const StepParams& p, const S* __restrict__ a, long long tstep) {
+  __shared__ double rho_c[kProbeCorners];
+  Ctl* c = p.ctl;
+  const long long rs = (long long)c->rec_start;
+  if (!c->dp_on || !c->rec_cap || tstep < rs || tstep - rs >= (long long)c->rec_cap) return;
+  const int tid = threadIdx.x;
+  if (tid < kProbeCorners) {
+    const int idx = c->probe_idx[tid];
+    double r = 0.0;
+    if (idx >= 0) {
+      double f[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld_cg(a + (size_t)i * p.ns + idx, i);
+      double jx, jy;
+      moments(f, r, jx, jy);
+    }
+    rho_c[tid] = r;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double wall[2];
+    for (int side = 0; side < 2; ++side) {
+      double pd[3];
+      for (int d = 0; d < 3; ++d) {
+        double sum = 0.0, wsum = 0.0;
+        for (int k = 0; k < 4; ++k) {
+          const int s = (side * 3 + d) * 4 + k;
+          if (c->probe_idx[s] < 0) continue;
+          sum += c->probe_w[s] * rho_c[s];
+          wsum += c->probe_w[s];
+        }
+        pd[d] = wsum > 0.0 ? sum / wsum : __longlong_as_double(0x7ff8000000000000ll);
+      }
+      wall[side] = 3.0 * pd[0] - 3.0 * pd[1] + pd[2];
+    }
+    c->hist[(size_t)(tstep - rs) * kRec + 9] = (1.0 / 3.0) * (wall[0] - wall[1]) / (c->u_ref * c->u_ref);
+  }
+  __syncthreads();
+}
+
+// Runs in the last link block to finish a step: reduces the force partials in a fixed order,
+// writes the step record, evaluates the pressure probe of the previous step (whose result is the
+// current `a`), advances the controls and t.
+template <class S>
+__device__ void step_epilogue(const StepParams& p, const S* __restrict__ a) {
   __shared__ double red[kBlock];
   __shared__ double res[2 * kMaxGroups];
-  __shared__ double rho_c[kProbeCorners];
   const int tid = threadIdx.x;
   Ctl* c = p.ctl;
   const int ncomp = 2 * p.ngroups;
-  // 1) force: each component summed over the link-block partials with a fixed stride pattern,
-  //    then a fixed shared-memory tree (one component at a time, to keep shared memory small).
+  // force: each component summed over the link-block partials with a fixed stride pattern, then
+  // a fixed shared-memory tree (one component at a time, to keep shared memory small).
   for (int k = 0; k < ncomp; ++k) {
     double acc = 0.0;
     for (int blk = tid; blk < p.nlink; blk += kBlock)
@@ -189,140 +238,149 @@ __device__ void step_epilogue(const StepParams& p, const S* __restrict__ b) {
     if (tid == 0) res[k] = red[0];
     __syncthreads();
   }
-  // 2) pressure-drop probe densities on the new state.
-  if (c->dp_on && tid < kProbeCorners) {
-    const int idx = c->probe_idx[tid];
-    double r = 0.0;
-    if (idx >= 0) {
-      R f[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) f[i] = Store<S>::ld_cg(b + (size_t)i * p.ns + idx, i);
-      double fd[9];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) fd[i] = (double)f[i];
-      double rr, jx, jy;
-      moments(fd, rr, jx, jy);
-      r = rr;
-    }
-    rho_c[tid] = r;
-  }
-  __syncthreads();
+  const unsigned long long t = c->t;
+  const bool commit = !c->dry;
+  if (commit) record_probe<S>(p, a, (long long)t - 1);
   if (tid == 0) {
-    const unsigned long long t = c->t;
-    bool finite = true;
-    for (int k = 0; k < 2 * kMaxGroups; ++k) {
-      const double v = k < ncomp ? res[k] : 0.0;
-      c->force[k] = v;
-      if (!isfinite(v)) finite = false;
-    }
-    if (!finite && !c->nonfinite) {
-      c->nonfinite = 1;
-      c->nonfinite_t = t;
-    }
-    double dp = 0.0;
-    if (c->dp_on) {
-      // probe_density (src/sim.rs:624-644) at distances 1, 2, 3 on each side, extrapolated
-      // (src/sim.rs:648-651); pressure drop of src/cases/cylinder.rs:272-277.
-      double wall[2];
-      for (int side = 0; side < 2; ++side) {
-        double pd[3];
-        for (int d = 0; d < 3; ++d) {
-          double sum = 0.0, wsum = 0.0;
-          for (int k = 0; k < 4; ++k) {
-            const int s = (side * 3 + d) * 4 + k;
-            if (c->probe_idx[s] < 0) continue;
-            sum += c->probe_w[s] * rho_c[s];
-            wsum += c->probe_w[s];
-          }
-          pd[d] = wsum > 0.0 ? sum / wsum : __longlong_as_double(0x7ff8000000000000ll);
-        }
-        wall[side] = 3.0 * pd[0] - 3.0 * pd[1] + pd[2];
+    if (commit) {
+      bool finite = true;
+      for (int k = 0; k < 2 * kMaxGroups; ++k) {
+        const double v = k < ncomp ? res[k] : 0.0;
+        c->force[k] = v;
+        if (!isfinite(v)) finite = false;
       }
-      dp = (1.0 / 3.0) * (wall[0] - wall[1]) / (c->u_ref * c->u_ref);
+      if (!finite && !c->nonfinite) {
+        c->nonfinite = 1;
+        c->nonfinite_t = t;
+      }
+      if (c->rec_cap && t >= c->rec_start && t - c->rec_start < c->rec_cap) {
+        double* r = c->hist + (size_t)(t - c->rec_start) * kRec;
+        for (int k = 0; k < 2 * kMaxGroups; ++k) r[k] = c->force[k];
+        r[8] = c->drho;
+        r[9] = 0.0;
+      }
+      if (c->sched_on) {
+        const Controls k = read_controls(c);
+        c->vscale[1] = k.vs[1];
+        c->vscale[2] = k.vs[2];
+        c->target = k.target;
+        c->has_target = k.has_target;
+      }
+      c->t = t + 1;
     }
-    if (c->rec_cap && t >= c->rec_start && t - c->rec_start < c->rec_cap) {
-      double* r = c->hist + (size_t)(t - c->rec_start) * kRec;
-      for (int k = 0; k < 2 * kMaxGroups; ++k) r[k] = c->force[k];
-      r[8] = c->drho;
-      r[9] = dp;
-    }
-    if (c->sched_on) {
-      const Controls k = read_controls(c);
-      c->vscale[1] = k.vs[1];
-      c->vscale[2] = k.vs[2];
-      c->target = k.target;
-      c->has_target = k.has_target;
-    }
-    c->t = t + 1;
     c->arrive = 0;
     __threadfence();
   }
 }
 
+// Link blocks publish their force partial and count themselves; the last one runs the epilogue.
 template <class S>
-__device__ __forceinline__ void arrive(const StepParams& p, const S* __restrict__ b) {
+__device__ __forceinline__ void arrive(const StepParams& p, const S* __restrict__ a) {
   __shared__ int last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned prev = atomicAdd(&p.ctl->arrive, 1u);
-    last = prev == (unsigned)(p.nbulk + p.nlink - 1);
+    last = prev == (unsigned)(p.nlink - 1);
   }
   __syncthreads();
   if (last) {
     __threadfence();
-    step_epilogue<S>(p, b);
+    step_epilogue<S>(p, a);
   }
 }
 
+// Records the pressure probe of the last step of a batch (its result is the current `a`).
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_probe(const __grid_constant__ StepParams p, const S* __restrict__ a) {
+  record_probe<S>(p, a, (long long)p.ctl->t - 1);
+}
+
 // ------------------------------------------------------------------ bulk kernel
+// Pull + collide for the interior nodes. Block t covers the kBlock consecutive cells of row tile
+// t. The nine population loads are issued together with the flag load, for every cell of the
+// tile (wrap keeps every neighbour index inside the grid), so no load waits for the flag; only
+// interior cells (flag 0) store. Boundary cells are written by the link kernel, solid cells never.
+template <class S>
+__device__ __forceinline__ void pull(const S* __restrict__ a, unsigned ns, int nx, int ny, int x, int y,
+                                     typename Store<S>::R* f) {
+  const int ym = y == 0 ? ny - 1 : y - 1;
+  const int yp = y == ny - 1 ? 0 : y + 1;
+  const int xm = x == 0 ? nx - 1 : x - 1;
+  const int xp = x == nx - 1 ? 0 : x + 1;
+  const unsigned rc = (unsigned)(y * nx), rm = (unsigned)(ym * nx), rp = (unsigned)(yp * nx);
+  f[0] = Store<S>::ld(a + rc + x, 0);
+  f[1] = Store<S>::ld(a + 1u * ns + rc + xm, 1);
+  f[2] = Store<S>::ld(a + 2u * ns + rm + x, 2);
+  f[3] = Store<S>::ld(a + 3u * ns + rc + xp, 3);
+  f[4] = Store<S>::ld(a + 4u * ns + rp + x, 4);
+  f[5] = Store<S>::ld(a + 5u * ns + rm + xm, 5);
+  f[6] = Store<S>::ld(a + 6u * ns + rm + xp, 6);
+  f[7] = Store<S>::ld(a + 7u * ns + rp + xp, 7);
+  f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
+}
+
 template <class S, int CK>
 __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepParams p,
                                                  const S* __restrict__ a, S* __restrict__ b) {
   using R = typename Store<S>::R;
   const int nx = p.nx, ny = p.ny;
-  const unsigned ns = p.ns;
+  const int y = blockIdx.x / p.tiles_per_row;
+  const int x = (blockIdx.x - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
+  if (x >= nx) return;
+  const unsigned idx = (unsigned)(y * nx + x);
+  const uint8_t fl = __ldg(p.flag + idx);
+  R f[9];
+  pull(a, p.ns, nx, ny, x, y, f);
   const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
-  for (int tile = blockIdx.x; tile < p.ntiles; tile += gridDim.x) {
-    const int y = tile / p.tiles_per_row;
-    const int x = (tile - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
-    if (x >= nx) continue;
-    const unsigned idx = (unsigned)(y * nx + x);
-    if (__ldg(p.flag + idx) != 0) continue;
-    const int ym = y == 0 ? ny - 1 : y - 1;
-    const int yp = y == ny - 1 ? 0 : y + 1;
-    const int xm = x == 0 ? nx - 1 : x - 1;
-    const int xp = x == nx - 1 ? 0 : x + 1;
-    const unsigned rc = (unsigned)(y * nx), rm = (unsigned)(ym * nx), rp = (unsigned)(yp * nx);
-    R f[9];
-    f[0] = Store<S>::ld(a + rc + x, 0);
-    f[1] = Store<S>::ld(a + 1u * ns + rc + xm, 1);
-    f[2] = Store<S>::ld(a + 2u * ns + rm + x, 2);
-    f[3] = Store<S>::ld(a + 3u * ns + rc + xp, 3);
-    f[4] = Store<S>::ld(a + 4u * ns + rp + x, 4);
-    f[5] = Store<S>::ld(a + 5u * ns + rm + xm, 5);
-    f[6] = Store<S>::ld(a + 6u * ns + rm + xp, 6);
-    f[7] = Store<S>::ld(a + 7u * ns + rp + xp, 7);
-    f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
-    if (CK == 2)
-      collide_forced(f, op, om, gx, gy);
-    else if (CK == 0)
-      collide_bgk(f, op);
-    else
-      collide_trt(f, op, om);
+  if (CK == 2)
+    collide_forced(f, op, om, gx, gy);
+  else if (CK == 0)
+    collide_bgk(f, op);
+  else
+    collide_trt(f, op, om);
+  if (fl != 0) return;
 #pragma unroll
-    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * ns + idx, i, f[i]);
-  }
-  arrive<S>(p, b);
+  for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * p.ns + idx, i, f[i]);
 }
 
 // ------------------------------------------------------------------ link kernel
+// One thread per boundary node. The node's link records are read as three 16-byte vectors each;
+// the force of each group is accumulated per thread in shared memory (in link order), then
+// reduced per block by a fixed tree.
+struct LinkView {
+  double q, cu6, uw0, uw1, rho;
+  int behind, dir, flags, vgroup, fgroup;
+};
+
+__device__ __forceinline__ LinkView load_link(const LinkRecDev* links, int l) {
+  const int4* v = reinterpret_cast<const int4*>(links + l);
+  const int4 w0 = __ldg(v), w1 = __ldg(v + 1), w2 = __ldg(v + 2);
+  LinkView L;
+  L.q = __hiloint2double(w0.y, w0.x);
+  L.cu6 = __hiloint2double(w0.w, w0.z);
+  L.uw0 = __hiloint2double(w1.y, w1.x);
+  L.uw1 = __hiloint2double(w1.w, w1.z);
+  L.rho = __hiloint2double(w2.y, w2.x);
+  L.behind = w2.z;
+  const unsigned packed = (unsigned)w2.w;  // dir, flags, vgroup, fgroup (little endian)
+  L.dir = (int)(packed & 0xffu);
+  L.flags = (int)((packed >> 8) & 0xffu);
+  L.vgroup = (int)((packed >> 16) & 0xffu);
+  L.fgroup = (int)(int8_t)(packed >> 24);
+  return L;
+}
+
+#ifndef VL_LINK_MIN_BLOCKS
+#define VL_LINK_MIN_BLOCKS 1
+#endif
 template <class S, int CK>
-__global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepParams p,
+__global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links(const __grid_constant__ StepParams p,
                                                   const S* __restrict__ a, S* __restrict__ b) {
   using R = typename Store<S>::R;
   __shared__ double s_un[kBlock];
   __shared__ double s_drho;
+  __shared__ double s_acc[2 * kMaxGroups][kBlock];
   __shared__ double s_red[2 * kMaxGroups][kBlock / 32];
   const int tid = threadIdx.x;
   const int nx = p.nx, ny = p.ny;
@@ -358,39 +416,35 @@ __global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepPa
     __syncthreads();
     drho = s_drho;
   }
-  if (blockIdx.x == 0 && tid == 0) p.ctl->drho = drho;
+  if (blockIdx.x == 0 && tid == 0 && !p.ctl->dry) p.ctl->drho = drho;
 
-  double acc[2 * kMaxGroups];
+  const bool forces = p.ngroups > 0;
+  if (forces) {
 #pragma unroll
-  for (int k = 0; k < 2 * kMaxGroups; ++k) acc[k] = 0.0;
+    for (int k = 0; k < 2 * kMaxGroups; ++k) s_acc[k][tid] = 0.0;
+  }
 
   const LinkRecDev* links = (const LinkRecDev*)p.links;
-  for (int k = blockIdx.x * kBlock + tid; k < p.nb; k += p.nlink * kBlock) {
+  const int k = blockIdx.x * kBlock + tid;
+  if (k < p.nb) {
     const int idx = __ldg(p.bnode_idx + k);
     const int first = __ldg(p.bnode_first + k), last = __ldg(p.bnode_first + k + 1);
     const int y = idx / nx, x = idx - y * nx;
-    const int ym = y == 0 ? ny - 1 : y - 1;
-    const int yp = y == ny - 1 ? 0 : y + 1;
-    const int xm = x == 0 ? nx - 1 : x - 1;
-    const int xp = x == nx - 1 ? 0 : x + 1;
-    const unsigned rc = (unsigned)(y * nx), rm = (unsigned)(ym * nx), rp = (unsigned)(yp * nx);
-    R f[9];
-    f[0] = Store<S>::ld(a + rc + x, 0);
-    f[1] = Store<S>::ld(a + 1u * ns + rc + xm, 1);
-    f[2] = Store<S>::ld(a + 2u * ns + rm + x, 2);
-    f[3] = Store<S>::ld(a + 3u * ns + rc + xp, 3);
-    f[4] = Store<S>::ld(a + 4u * ns + rp + x, 4);
-    f[5] = Store<S>::ld(a + 5u * ns + rm + xm, 5);
-    f[6] = Store<S>::ld(a + 6u * ns + rm + xp, 6);
-    f[7] = Store<S>::ld(a + 7u * ns + rp + xp, 7);
-    f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
+    // The incoming populations (pulled from the neighbours) and the node's own post-collision
+    // populations: every per-link read of the reference's link pass other than the node behind
+    // the link (a[j][idx], a[i][idx], the node velocity) is one of the own values, so the link
+    // loop below touches memory only for its record and that one node.
+    R f[9], own[9];
+    pull(a, ns, nx, ny, x, y, f);
+#pragma unroll
+    for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
     bool have_u = false;
     R ux = R(0), uy = R(0);
     for (int l = first; l < last; ++l) {
-      const LinkRecDev L = links[l];
+      const LinkView L = load_link(links, l);
       const int j = L.dir;
       const int i = opp_of(j);
-      const R out = Store<S>::ld(a + (unsigned)j * ns + idx, j);
+      const R out = pick(own, j);
       const R scale = (R)ctl.vs[L.vgroup];
       R back;
       if (!(L.flags & 1)) {
@@ -399,7 +453,7 @@ __global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepPa
         const R q = (R)L.q;
         if (q >= R(0.5)) {
           const R kq = R(0.5) / q;
-          back = kq * (out - corr) + (R(1.0) - kq) * Store<S>::ld(a + (unsigned)i * ns + idx, i);
+          back = kq * (out - corr) + (R(1.0) - kq) * pick(own, i);
         } else if (L.behind >= 0) {
           back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * Store<S>::ld(a + (unsigned)j * ns + (unsigned)L.behind, j) - corr;
         } else {
@@ -409,11 +463,8 @@ __global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepPa
         // Open boundary: anti-bounce-back around the equilibrium of the boundary density
         // (src/sim.rs:480-488), with the node's own velocity.
         if (!have_u) {
-          R g[9];
-#pragma unroll
-          for (int d = 0; d < 9; ++d) g[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
           R rho, jx, jy;
-          moments(g, rho, jx, jy);
+          moments(own, rho, jx, jy);
           ux = jx / rho - R(0.5) * gx;
           uy = jy / rho - R(0.5) * gy;
           have_u = true;
@@ -433,9 +484,8 @@ __global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepPa
         // Galilean-invariant momentum exchange (src/sim.rs:490-495), accumulated in FP64.
         const double o = (double)out, bk = (double)back;
         const double wux = L.uw0 * (double)scale, wuy = L.uw1 * (double)scale;
-        const double fxc = (double)cx_of(j) * (o + bk) - wux * (o - bk);
-        const double fyc = (double)cy_of(j) * (o + bk) - wuy * (o - bk);
-        add_group(acc, L.fgroup, fxc, fyc);
+        s_acc[2 * L.fgroup][tid] += (double)cx_of(j) * (o + bk) - wux * (o - bk);
+        s_acc[2 * L.fgroup + 1][tid] += (double)cy_of(j) * (o + bk) - wuy * (o - bk);
       }
     }
     if (CK == 2)
@@ -449,23 +499,22 @@ __global__ void __launch_bounds__(kBlock) k_links(const __grid_constant__ StepPa
   }
 
   // Block partial of the force: fixed shuffle tree within each warp, then fixed order over warps.
-  if (p.ngroups > 0) {
+  if (forces) {
     const int lane = tid & 31, warp = tid >> 5;
-#pragma unroll
-    for (int k = 0; k < 2 * kMaxGroups; ++k) {
-      double v = acc[k];
+    for (int c = 0; c < 2 * p.ngroups; ++c) {
+      double v = s_acc[c][tid];
 #pragma unroll
       for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) s_red[k][warp] = v;
+      if (lane == 0) s_red[c][warp] = v;
     }
     __syncthreads();
-    if (tid < 2 * kMaxGroups) {
+    if (tid < 2 * p.ngroups) {
       double v = 0.0;
       for (int w = 0; w < kBlock / 32; ++w) v += s_red[tid][w];
       p.partials[(size_t)blockIdx.x * (2 * kMaxGroups) + tid] = v;
     }
   }
-  arrive<S>(p, b);
+  arrive<S>(p, a);
 }
 
 // ------------------------------------------------------------------ utility kernels

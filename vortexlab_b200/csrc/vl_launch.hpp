@@ -24,8 +24,8 @@ struct Launchers {
   cudaError_t (*reduce)(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,
                         double* out, int blocks, cudaStream_t s);
   cudaError_t (*gather)(int m, unsigned ns, const int32_t* cells, const void* a, double* out, cudaStream_t s);
-  // Resident blocks per SM of the bulk kernel (for grid sizing).
-  int (*bulk_occupancy)(int ck);
+  // Records the pressure probe of the last step of a batch (one block).
+  cudaError_t (*probe)(const StepParams& p, const void* a, cudaStream_t s);
 };
 
 const Launchers& launchers_f64();

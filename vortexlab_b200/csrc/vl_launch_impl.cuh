@@ -12,7 +12,7 @@ struct LaunchImpl {
   // (a step launched in two halves, for per-kernel timing).
   template <int CK>
   static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which) {
-    if ((which & 1) && p.nlink > 0) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
+    if (which & 1) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
     if (which & 2) k_bulk<S, CK><<<p.nbulk, kBlock, 0, s>>>(p, a, b);
     return cudaGetLastError();
   }
@@ -57,18 +57,12 @@ struct LaunchImpl {
     k_gather<S><<<(m + 127) / 128, 128, 0, s>>>(m, ns, cells, (const S*)a, out);
     return cudaGetLastError();
   }
-  static int bulk_occupancy(int ck) {
-    int blocks = 0;
-    cudaError_t e;
-    switch (ck) {
-      case 0: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 0>, kBlock, 0); break;
-      case 2: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 2>, kBlock, 0); break;
-      default: e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k_bulk<S, 1>, kBlock, 0); break;
-    }
-    return (e == cudaSuccess && blocks > 0) ? blocks : 1;
+  static cudaError_t probe(const StepParams& p, const void* a, cudaStream_t s) {
+    k_probe<S><<<1, kBlock, 0, s>>>(p, (const S*)a);
+    return cudaGetLastError();
   }
   static const Launchers& table() {
-    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &bulk_occupancy};
+    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &probe};
     return t;
   }
 };
