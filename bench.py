@@ -27,9 +27,10 @@ sys.path.insert(0, ROOT)
 BOX = dict(nx=8192, ny=4096, seed=0x5EED0001, fraction=0.05, tau=0.55, u=0.05)
 BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36}
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes per fluid-node update of the bulk kernel from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch divided by the interior nodes it updates), per precision.
-NCU_DRAM_BYTES_PER_LU = {}
+# DRAM bytes per interior-node update of the bulk kernel from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch of the 2048 x 2048 box divided by its interior nodes; see
+# profiles/k_bulk_k_links_f64_disk_box.md), per precision. Scaled to a full launch by nodes.
+NCU_DRAM_BYTES_PER_LU = {"f64": 139.3}
 
 
 def workload_name(prec):

@@ -35,7 +35,7 @@ extern "C" {
 #define VL_OK 0
 #define VL_EINVAL (-1)       /* contract violation (the reference panics)                      */
 #define VL_ECUDA (-2)        /* CUDA runtime error or no CUDA device                           */
-#define VL_EDIVERGED (-3)    /* non-finite force: src/cases/cylinder.rs:397-404, tunnel.rs:78-84 */
+#define VL_EDIVERGED (-3)    /* non-finite force: src/cases/cylinder.rs:179-186, tunnel.rs:78-84 */
 #define VL_ENOMEM (-4)       /* device or host allocation failed                               */
 #define VL_EUNSUPPORTED (-5) /* valid request that this build does not implement               */
 
@@ -152,7 +152,7 @@ int vl_sim_outlet_density_offset(vl_sim* s, double* out);                 /* pub
 int vl_sim_t(vl_sim* s, uint64_t* t);                                      /* pub t :214 */
 /* Divergence check: nonfinite = 1 once a step produced a non-finite force, with the step index
  * (t before that step). The reference's cases test `!cd.is_finite()` after every step
- * (src/cases/cylinder.rs:397-404, src/cases/tunnel.rs:78-84); here the device records it. */
+ * (src/cases/cylinder.rs:179-186, src/cases/tunnel.rs:78-84); here the device records it. */
 int vl_sim_status(vl_sim* s, int* nonfinite, uint64_t* first_t);
 /* pub force :198 — force[g] = (fx, fy) of the last step; out holds 2 * ngroups doubles. */
 int vl_sim_force(vl_sim* s, double* out);
@@ -177,7 +177,7 @@ int vl_sim_state_hash(vl_sim* s, uint64_t* out);                           /* :6
  *   [8]  outlet density offset used in that step
  *   [9]  pressure-drop probe value after that step (see vl_sim_set_dp_probe), else 0
  * Replaces the per-step host reads of Channel::coefficients (src/cases/channel.rs:133-136) and
- * Rig::pressure_drop (src/cases/cylinder.rs:272-277). */
+ * Rig::pressure_drop (src/cases/cylinder.rs:54-59). */
 #define VL_REC 10
 int vl_sim_record(vl_sim* s, uint64_t capacity);   /* 0 disables; (re)starts at the next step */
 int vl_sim_history(vl_sim* s, double* out, uint64_t* count);  /* out: count * VL_REC doubles */

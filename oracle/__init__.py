@@ -492,7 +492,7 @@ class Channel:
     def run(self, steps, record_force=True, dp_probe=None):
         """Runs `steps` Channel::step calls. Returns (force history (steps, 2) | None, dp | None).
 
-        dp_probe = (xc, yc, r) records the cylinder pressure drop (src/cases/cylinder.rs:272-277).
+        dp_probe = (xc, yc, r) records the cylinder pressure drop (src/cases/cylinder.rs:54-59).
         """
         fh = np.zeros((steps, 2)) if record_force else None
         dp = np.zeros(steps) if dp_probe is not None else None
@@ -511,7 +511,7 @@ class Channel:
 
 
 def cylinder_rig(n, u_mean=0.05, re=100.0, collision=TRT, ramp_units=8.0, threads=1):
-    """src/cases/cylinder.rs:253-268. Returns (channel, n, xc, yc)."""
+    """src/cases/cylinder.rs:35-50. Returns (channel, n, xc, yc)."""
     nf = float(n)
     xc = yc = 0.5 + 2.0 * nf
     nu = u_mean * nf / re

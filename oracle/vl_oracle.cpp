@@ -18,7 +18,7 @@
 //
 // Files restated: src/lattice.rs:16-156, src/sim.rs:33-735, src/geometry.rs:11-279,
 // src/pool.rs (row split only), src/cases/mod.rs:10-18, src/cases/channel.rs:22-189,
-// src/cases/cylinder.rs:236-450, src/cases/tunnel.rs:11-67, src/cases/poiseuille.rs:11-21,
+// src/cases/cylinder.rs:18-232, src/cases/tunnel.rs:11-67, src/cases/poiseuille.rs:11-21,
 // src/signal.rs:6-147.
 
 #include <algorithm>
@@ -1330,7 +1330,7 @@ void vlo_channel_set_absorbing(void* c, int on) { ((Channel*)c)->absorbing_outle
 double vlo_channel_u_ref(void* c) { return ((Channel*)c)->u_ref; }
 // Runs `steps` Channel::step calls. If `force_hist` is non-null it receives force[0] (fx, fy)
 // after each step. If `dp_hist` is non-null it receives the cylinder pressure drop of
-// src/cases/cylinder.rs:272-277 for a body centred at (xc, yc) with radius r.
+// src/cases/cylinder.rs:54-59 for a body centred at (xc, yc) with radius r.
 void vlo_channel_run(void* c, uint64_t steps, double* force_hist, double* dp_hist, double xc,
                      double yc, double r) {
   auto ch = (Channel*)c;

@@ -1075,7 +1075,7 @@ int vl_sim_set_dp_probe(vl_sim* s, double xc, double yc, double r, double u_ref)
   int rc = s->pull_ctl();
   if (rc) return rc;
   // Front wall point (xc - r, yc) with outward normal (-1, 0), back (xc + r, yc) with (1, 0);
-  // samples at distances 1, 2, 3 (src/sim.rs:648-651, src/cases/cylinder.rs:272-277).
+  // samples at distances 1, 2, 3 (src/sim.rs:648-651, src/cases/cylinder.rs:54-59).
   const double wx[2] = {xc - r, xc + r}, nxv[2] = {-1.0, 1.0};
   for (int side = 0; side < 2; ++side)
     for (int d = 0; d < 3; ++d) {

@@ -169,7 +169,7 @@ __device__ __forceinline__ Controls read_controls(const Ctl* c) {
 }
 
 // ------------------------------------------------------------------ epilogue
-// Pressure-drop probe (src/cases/cylinder.rs:272-277) of the state `a` recorded as step `tstep`
+// Pressure-drop probe (src/cases/cylinder.rs:54-59) of the state `a` recorded as step `tstep`
 // of the history: probe_density (src/sim.rs:624-644) at distances 1, 2, 3 from each wall point,
 // extrapolated to the wall (src/sim.rs:648-651). Block-wide; every thread must call it.
 template <class S>

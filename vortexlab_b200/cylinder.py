@@ -3,7 +3,7 @@
 Channel 22n x 4.1n cells (n cells per diameter), cylinder of diameter n at (2n + 1/2, 2n + 1/2),
 parabolic inflow with mean velocity ``u_mean``, TRT by default. Forces and the pressure drop are
 recorded on the device every step and downloaded once (the reference reads them on the host after
-every step, src/cases/cylinder.rs:394-408).
+every step, src/cases/cylinder.rs:176-190).
 """
 from __future__ import annotations
 
@@ -18,7 +18,7 @@ from . import TRT, Channel, Circle, Collision, Inflow, Series, Spec, VortexError
 
 @dataclass
 class Setup:
-    """src/cases/cylinder.rs:236-244."""
+    """src/cases/cylinder.rs:18-26."""
 
     n: int
     u_mean: float = 0.05
@@ -35,7 +35,7 @@ class Rig:
     yc: float
 
     def pressure_drop(self) -> float:
-        """src/cases/cylinder.rs:272-277, from the current state."""
+        """src/cases/cylinder.rs:54-59, from the current state."""
         r = 0.5 * self.n
         front = self.ch.sim.probe_density_at_wall(self.xc - r, self.yc, -1.0, 0.0)
         back = self.ch.sim.probe_density_at_wall(self.xc + r, self.yc, 1.0, 0.0)
@@ -43,7 +43,7 @@ class Rig:
 
 
 def rig(s: Setup, re: float, ramp_units: float) -> Rig:
-    """src/cases/cylinder.rs:253-268."""
+    """src/cases/cylinder.rs:35-50."""
     if s.n < 10 or s.n % 10 != 0:
         raise ValueError("cells per diameter must be a multiple of 10")
     n = float(s.n)
@@ -55,7 +55,7 @@ def rig(s: Setup, re: float, ramp_units: float) -> Rig:
 
 @dataclass
 class Unsteady:
-    """src/cases/cylinder.rs:360-383."""
+    """src/cases/cylinder.rs:142-165."""
 
     n: int
     cd_max: float
@@ -94,7 +94,7 @@ def run_record(r: Rig, steps: int, chunk: int = 1 << 16):
 
 
 def run_2d2(s: Setup, total_units: float, window_units: float) -> Unsteady:
-    """Case 2D-2 (Re = 100), src/cases/cylinder.rs:387-438. Raises VortexError on divergence."""
+    """Case 2D-2 (Re = 100), src/cases/cylinder.rs:169-220. Raises VortexError on divergence."""
     start = time.time()
     r = rig(s, 100.0, 8.0)
     unit = r.n / s.u_mean
@@ -122,7 +122,7 @@ def run_2d2(s: Setup, total_units: float, window_units: float) -> Unsteady:
 
 
 def bench(s: Setup, steps: int):
-    """src/cases/cylinder.rs:442-450: times ``steps`` steps (forces every step). Returns
+    """src/cases/cylinder.rs:224-232: times ``steps`` steps (forces every step). Returns
     (channel, seconds) with the device time of the batch."""
     r = rig(s, 100.0, 8.0)
     r.ch.step(steps)
