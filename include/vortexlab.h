@@ -203,6 +203,28 @@ int vl_sim_autotune(vl_sim* s, int steps_each, double* ms3);
 /* Number of kernel launches issued by this sim so far (steps launch one or two kernels each). */
 int vl_sim_launch_count(vl_sim* s, uint64_t* out);
 
+/* ---- allocation-free reduction
+ * No counterpart in the reference. Total mass, total momentum and largest speed (the quantities
+ * of vl_sim_total_mass / vl_sim_total_momentum / vl_sim_max_speed) of a population array that the
+ * caller owns, for callers that cannot allocate device memory: a host framework that hands out
+ * every device byte from its own pool, a plugin that may only touch the buffers it is given, code
+ * running where cudaMalloc is not allowed. The call allocates nothing: its per-block partial sums
+ * live in a fixed array inside this library (112 KB held on every GPU that loads it, until the
+ * process exits).
+ *   populations  device pointer, FP64, population i of cell idx at i * plane_stride + idx
+ *   flag         device pointer, one byte per cell (2 = not fluid, skipped), as vl_sim_flags
+ *   n            cells, at most VL_REDUCE_STATIC_MAX_CELLS (larger n: VL_EINVAL)
+ *   gx, gy       body acceleration (the speed is that of Sim::macros)
+ *   out4         device pointer to 4 doubles: mass, momentum x, momentum y, largest speed
+ *   stream       cudaStream_t to run on (NULL: the default stream); returns before completion
+ * The first call on a device looks up the array's device address (once per device, with that
+ * device current); make that first call before any stream capture. Every call reuses the same
+ * array and overwrites each slot it reads, so nothing needs clearing, but calls whose kernels
+ * overlap on the GPU (other streams, other host threads) race on it. */
+#define VL_REDUCE_STATIC_MAX_CELLS 33554432
+int vl_reduce_f64_static(const double* populations, size_t plane_stride, const uint8_t* flag, size_t n,
+                         double gx, double gy, double* out4, void* stream);
+
 /* ================================================================ channel: src/cases/channel.rs */
 /* Spec :47-58 plus Kick :37-45. `body` is owned by the channel after the call. */
 typedef struct {

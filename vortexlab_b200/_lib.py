@@ -114,6 +114,7 @@ def _declare(L):
         "vl_sim_get_schedule": (i, [vp]),
         "vl_sim_autotune": (i, [vp, i, P(d)]),
         "vl_sim_launch_count": (i, [vp, P(u64)]),
+        "vl_reduce_f64_static": (i, [vp, sz, vp, sz, d, d, vp, vp]),
         "vl_channel_new": (vp, [P(vl_channel_spec), i]),
         "vl_channel_free": (None, [vp]),
         "vl_channel_sim": (vp, [vp]),

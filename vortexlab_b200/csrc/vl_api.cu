@@ -54,6 +54,8 @@ constexpr int kReduceBlocks = 296;
 
 }  // namespace
 
+int vl::set_error(int code, const char* msg) { return fail(code, msg); }
+
 // ==================================================================== device-resident sim
 struct vl_sim {
   int device = 0;

@@ -28,6 +28,9 @@ struct Launchers {
   cudaError_t (*probe)(const StepParams& p, const void* a, cudaStream_t s);
 };
 
+// Records a failure for vl_last_error / vl_last_status (thread-local) and returns `code`.
+int set_error(int code, const char* msg);
+
 const Launchers& launchers_f64();
 const Launchers& launchers_f32();
 const Launchers& launchers_f16s();
