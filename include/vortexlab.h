@@ -251,6 +251,42 @@ int vl_channel_step(vl_channel* c, uint64_t steps);
 int vl_channel_coefficients(vl_channel* c, double d, double* cd, double* cl); /* :133-136 */
 double vl_channel_u_ref(const vl_channel* c);
 
+/* ================================================================ batched tunnels
+ * No single reference counterpart: the reference runs one Channel at a time
+ * (src/cases/tunnel.rs:52-92). A batch advances many channels of uneven sizes, shapes and Reynolds
+ * numbers together on one device, each for its own number of steps; every tunnel follows
+ * Channel::step exactly (a tunnel in a batch is bit-identical to the same tunnel run alone). */
+typedef struct vl_batch vl_batch;
+vl_batch* vl_batch_new(int precision);
+void vl_batch_free(vl_batch* b);
+/* Adds a channel (takes spec->body) to be run for `steps` steps; returns its index. */
+int vl_batch_add_channel(vl_batch* b, const vl_channel_spec* spec, uint64_t steps);
+/* Packs every tunnel into one device arena and starts them (t = 0). */
+int vl_batch_build(vl_batch* b);
+int vl_batch_size(const vl_batch* b);
+int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_t* fluid_nodes, uint64_t* steps);
+/* Bulk tile shape: 2^log2_tx cells x ty rows = 256 cells (32 <= 2^log2_tx <= 256). */
+int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty);
+int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty);
+int vl_batch_set_schedule(vl_batch* b, int schedule);  /* VL_SCHEDULE_* */
+/* Times the tile shapes 256x1, 128x2, 64x4, 32x8 on the current state without advancing it and
+ * keeps the fastest; ms4 (may be NULL) receives milliseconds per step for each. */
+int vl_batch_autotune(vl_batch* b, int steps_each, double* ms4);
+/* Runs every unfinished tunnel until it has done its steps (max_steps = 0), or at most max_steps
+ * global steps. Synchronous. */
+int vl_batch_run(vl_batch* b, uint64_t max_steps);
+int vl_batch_last_run_ms(vl_batch* b, float* ms);
+int vl_batch_global_step(const vl_batch* b, uint64_t* s);
+int vl_batch_launch_count(const vl_batch* b, uint64_t* out);
+/* Steps done, divergence flag and the last force (fx, fy) of tunnel k. */
+int vl_batch_status(vl_batch* b, int k, uint64_t* t, int* nonfinite, double* force2);
+/* Force (fx, fy) of tunnel k after each of its steps so far: 2 * count doubles. */
+int vl_batch_force_history(vl_batch* b, int k, double* out, uint64_t* count);
+/* FP64 populations of tunnel k (reference layout, 9 * nx * ny values), its flags, its state hash. */
+int vl_batch_download(vl_batch* b, int k, double* out);
+int vl_batch_flags(vl_batch* b, int k, uint8_t* out);
+int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
+
 /* ================================================================ signal: src/signal.rs */
 int vl_fft(double* re, double* im, size_t n);                              /* :6-44 */
 double vl_mean(const double* x, size_t n);                                 /* :61-63 */

@@ -47,6 +47,7 @@ def _sources(defines=()):
         ("vl_api.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_api.cu")]),
         ("vl_step_f64.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_step_f64.cu")]),
         ("vl_step_lp.o", [nvcc] + cu_flags + inc + ["-c", os.path.join(CSRC, "vl_step_lp.cu")]),
+        ("vl_batch.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_batch.cu")]),
         ("vl_noalloc.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_noalloc.cu")]),
     ]
     return jobs

@@ -122,6 +122,25 @@ def _declare(L):
         "vl_channel_step": (i, [vp, u64]),
         "vl_channel_coefficients": (i, [vp, d, P(d), P(d)]),
         "vl_channel_u_ref": (d, [vp]),
+        "vl_batch_new": (vp, [i]),
+        "vl_batch_free": (None, [vp]),
+        "vl_batch_add_channel": (i, [vp, P(vl_channel_spec), u64]),
+        "vl_batch_build": (i, [vp]),
+        "vl_batch_size": (i, [vp]),
+        "vl_batch_tunnel_info": (i, [vp, i, P(sz), P(sz), P(sz), P(u64)]),
+        "vl_batch_set_tile": (i, [vp, i, i]),
+        "vl_batch_get_tile": (i, [vp, P(i), P(i)]),
+        "vl_batch_set_schedule": (i, [vp, i]),
+        "vl_batch_autotune": (i, [vp, i, P(d)]),
+        "vl_batch_run": (i, [vp, u64]),
+        "vl_batch_last_run_ms": (i, [vp, P(f)]),
+        "vl_batch_global_step": (i, [vp, P(u64)]),
+        "vl_batch_launch_count": (i, [vp, P(u64)]),
+        "vl_batch_status": (i, [vp, i, P(u64), P(i), P(d)]),
+        "vl_batch_force_history": (i, [vp, i, P(d), P(u64)]),
+        "vl_batch_download": (i, [vp, i, P(d)]),
+        "vl_batch_flags": (i, [vp, i, P(C.c_uint8)]),
+        "vl_batch_state_hash": (i, [vp, i, P(u64)]),
         "vl_fft": (i, [P(d), P(d), sz]),
         "vl_mean": (d, [P(d), sz]),
         "vl_rms": (d, [P(d), sz]),

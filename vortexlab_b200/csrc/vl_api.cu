@@ -13,11 +13,9 @@
 #include "../../include/vortexlab.h"
 #include "vl_device.cuh"
 #include "vl_host.hpp"
+#include "vl_internal.hpp"
 #include "vl_launch.hpp"
 
-struct vl_shape {
-  std::unique_ptr<vl::Shape> s;
-};
 struct vl_builder {
   vl::DomainSpec spec;
 };
@@ -1131,18 +1129,16 @@ struct vl_channel {
   ~vl_channel() { delete sim; }
 };
 
-extern "C" {
-
-vl_channel* vl_channel_new(const vl_channel_spec* sp, int precision) {
-  if (!sp) { fail(VL_EINVAL, "null spec"); return nullptr; }
-  std::unique_ptr<vl::Shape> body;
-  if (sp->body) { body = std::move(sp->body->s); delete sp->body; }
-  if (!body) { fail(VL_EINVAL, "channel needs a body shape"); return nullptr; }
+// Everything Channel::new and Channel::step decide on the host (src/cases/channel.rs:71-130): the
+// compiled domain, whether to start from the inflow profile, and the per-step control schedule
+// (inlet ramp, body kick) up to the step after which both are constant.
+int vl::plan_channel(const vl_channel_spec* sp, std::unique_ptr<vl::Shape> body, ChannelPlan& out) {
+  if (!body) return fail(VL_EINVAL, "channel needs a body shape");
   const size_t nx = sp->nx, ny = sp->ny;
-  if (nx < 3 || ny < 3) { fail(VL_EINVAL, "grid must be at least 3 x 3"); return nullptr; }
-  if (sp->inflow < 0 || sp->inflow > 2) { fail(VL_EINVAL, "unknown inflow"); return nullptr; }
-  // Channel::new (src/cases/channel.rs:71-116): inlet (moving wall, vgroup 1) at x = 0, outlet
-  // (pressure 1) at x = nx-1, side walls, body (vgroup 2, force group 0).
+  if (nx < 3 || ny < 3) return fail(VL_EINVAL, "grid must be at least 3 x 3");
+  if (sp->inflow < 0 || sp->inflow > 2) return fail(VL_EINVAL, "unknown inflow");
+  // Inlet (moving wall, vgroup 1) at x = 0, outlet (pressure 1) at x = nx-1, side walls, body
+  // (vgroup 2, force group 0).
   const double h = (double)(ny - 2);
   vl::DomainSpec spec;
   spec.nx = nx;
@@ -1205,40 +1201,63 @@ vl_channel* vl_channel_new(const vl_channel_spec* sp, int precision) {
       for (size_t x = 0; x < nx; ++x)
         if (shape.inside((double)x, (double)y)) spec.paint[y * nx + x] = k_b;
   }
-  vl::CompiledDomain dom;
   std::string err;
-  if (!vl::compile_domain(spec, dom, err)) { fail(VL_EINVAL, err); return nullptr; }
-  vl_sim* sim = make_sim(std::move(dom), precision);
-  if (!sim) return nullptr;
-  auto ch = std::make_unique<vl_channel>();
-  ch->sim = sim;
-  ch->u_ref = sp->u;
-  ch->ramp_steps = sp->ramp_steps;
-  if (sp->ramp_steps == 0) {
-    // Start from the developed inflow profile (src/cases/channel.rs:108-110).
-    std::vector<double> rho(sim->n, 1.0), ux(sim->n), uy(sim->n, 0.0);
-    for (size_t y = 0; y < ny; ++y) {
-      double u, v;
-      profile.at(0.0, (double)y, u, v);
-      for (size_t x = 0; x < nx; ++x) ux[y * nx + x] = u;
-    }
-    if (vl_sim_init(sim, rho.data(), ux.data(), uy.data(), 1.0, 0.0, 0.0) != VL_OK) return nullptr;
-  }
-  // Per-step controls (src/cases/channel.rs:118-130): inlet ramp and body kick, precomputed for
-  // every step until both are constant (ramp 1, kick 0), then uploaded once.
+  if (!vl::compile_domain(spec, out.dom, err)) return fail(VL_EINVAL, err);
+  out.u_ref = sp->u;
+  out.init_profile = sp->ramp_steps == 0;
+  out.profile = profile;
   uint64_t len = sp->ramp_steps;
   if (sp->has_kick) len = std::max<uint64_t>(len, sp->kick_start + sp->kick_duration);
-  std::vector<double> sched(2 * std::max<uint64_t>(len, 1));
+  out.sched_len = len;
+  out.sched.assign(2 * std::max<uint64_t>(len, 1), 0.0);
   for (uint64_t t = 0; t < len; ++t) {
-    sched[2 * t] = vl_ramp(t, sp->ramp_steps);
+    out.sched[2 * t] = vl_ramp(t, sp->ramp_steps);
     double v2 = 0.0;
     if (sp->has_kick && t >= sp->kick_start && t < sp->kick_start + sp->kick_duration) {
       const double s = (double)(t - sp->kick_start) / (double)sp->kick_duration;
       const double a = std::sin(M_PI * s);
       v2 = sp->kick_omega * (a * a) * std::copysign(1.0, std::sin(2.0 * M_PI * s));
     }
-    sched[2 * t + 1] = v2;
+    out.sched[2 * t + 1] = v2;
   }
+  return VL_OK;
+}
+
+// The inflow profile as (rho, ux, uy) arrays for a start from the developed inflow
+// (src/cases/channel.rs:108-110).
+void vl::profile_field(const ChannelPlan& plan, std::vector<double>& rho, std::vector<double>& ux,
+                       std::vector<double>& uy) {
+  const size_t nx = plan.dom.nx, ny = plan.dom.ny;
+  rho.assign(nx * ny, 1.0);
+  ux.assign(nx * ny, 0.0);
+  uy.assign(nx * ny, 0.0);
+  for (size_t y = 0; y < ny; ++y) {
+    double u, v;
+    plan.profile.at(0.0, (double)y, u, v);
+    for (size_t x = 0; x < nx; ++x) ux[y * nx + x] = u;
+  }
+}
+
+extern "C" {
+
+vl_channel* vl_channel_new(const vl_channel_spec* sp, int precision) {
+  if (!sp) { fail(VL_EINVAL, "null spec"); return nullptr; }
+  std::unique_ptr<vl::Shape> body;
+  if (sp->body) { body = std::move(sp->body->s); delete sp->body; }
+  vl::ChannelPlan plan;
+  if (vl::plan_channel(sp, std::move(body), plan) != VL_OK) return nullptr;
+  const vl::ChannelPlan& pl = plan;
+  std::vector<double> rho, ux, uy;
+  if (pl.init_profile) vl::profile_field(pl, rho, ux, uy);
+  const std::vector<double> sched = pl.sched;
+  const uint64_t len = pl.sched_len;
+  vl_sim* sim = make_sim(std::move(plan.dom), precision);
+  if (!sim) return nullptr;
+  auto ch = std::make_unique<vl_channel>();
+  ch->sim = sim;
+  ch->u_ref = sp->u;
+  ch->ramp_steps = sp->ramp_steps;
+  if (!rho.empty() && vl_sim_init(sim, rho.data(), ux.data(), uy.data(), 1.0, 0.0, 0.0) != VL_OK) return nullptr;
   if (cudaMalloc(&sim->d_sched, sched.size() * sizeof(double)) != cudaSuccess ||
       cudaMemcpy(sim->d_sched, sched.data(), sched.size() * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
     fail(VL_ECUDA, "schedule upload");

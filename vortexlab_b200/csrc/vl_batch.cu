@@ -1,0 +1,558 @@
+// Batched tunnels (C ABI vl_batch_*): many channels of uneven sizes, shapes and Reynolds numbers
+// advanced together on one device, each for its own number of steps.
+//
+// Global step s advances every tunnel that still has steps to run. Between the steps at which some
+// tunnel finishes, the set of active tunnels is fixed: that stretch ("segment") uses one tile list
+// and one link-chunk list and is replayed from a captured CUDA graph of 32 steps. Each step is the
+// batched link kernel (on a forked stream) and the batched bulk kernel, as for a single sim.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/vortexlab.h"
+#include "vl_batch.cuh"
+#include "vl_internal.hpp"
+#include "vl_launch.hpp"
+
+namespace {
+
+int fail(int code, const std::string& m) { return vl::set_error(code, m.c_str()); }
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(e == cudaErrorMemoryAllocation ? VL_ENOMEM : VL_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define VB_CUDA(call)                                   \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+  } while (0)
+
+constexpr int kGraphSteps = 32;
+
+template <class T>
+int upload(T** dst, const std::vector<T>& v) {
+  const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+  VB_CUDA(cudaMalloc((void**)dst, bytes));
+  if (!v.empty()) VB_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return VL_OK;
+}
+
+}  // namespace
+
+struct vl_batch {
+  int device = 0;
+  int prec = VL_F32;
+  const vl::Launchers* L = nullptr;
+  std::vector<vl::ChannelPlan> plans;
+  std::vector<uint64_t> steps;
+  bool built = false;
+  std::vector<vl::BatchTunnel> tun;
+  std::vector<int4> chunks_all;          // every chunk, tunnel-major
+  std::vector<int> chunk_first;          // first chunk of each tunnel in chunks_all
+  void* buf[2] = {nullptr, nullptr};
+  uint8_t* d_flag = nullptr;
+  int32_t* d_bidx = nullptr;
+  int32_t* d_bfirst = nullptr;
+  vl::LinkRecDev* d_links = nullptr;
+  int32_t* d_pidx = nullptr;
+  int8_t* d_pn = nullptr;
+  double* d_sched = nullptr;
+  vl::BatchTunnel* d_tun = nullptr;
+  vl::BatchState* d_st = nullptr;
+  int4* d_tiles = nullptr;
+  size_t tiles_cap = 0;
+  int4* d_chunks = nullptr;
+  double* d_partials = nullptr;
+  double* d_hist = nullptr;
+  cudaStream_t stream = nullptr, aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev0 = nullptr, ev1 = nullptr;
+  vl::BatchParams P{};
+  int ntiles = 0, nchunks = 0;
+  int schedule = 0;
+  int log2_tx = 8, ty = 1;
+  uint64_t s = 0;
+  uint64_t launches = 0;
+  cudaGraphExec_t gexec = nullptr;
+  std::vector<int4> tiles_h, chunks_h;   // host copies of the current work lists
+  bool timed = false;
+
+  ~vl_batch() {
+    cudaSetDevice(device);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_sched,
+                    d_tun, d_st, d_tiles, d_chunks, d_partials, d_hist};
+    for (void* p : ptrs)
+      if (p) cudaFree(p);
+    cudaEvent_t evs[] = {ev_fork, ev_join, ev0, ev1};
+    for (cudaEvent_t e : evs)
+      if (e) cudaEventDestroy(e);
+    if (aux) cudaStreamDestroy(aux);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  const void* a() const { return buf[s & 1]; }
+  void* b() const { return buf[(s & 1) ^ 1]; }
+  void* tunnel_ptr(void* base, int k) const { return (char*)base + tun[k].pop_off * L->elem; }
+
+  // Work lists of the tunnels active at global step s (the ones with steps left).
+  int build_lists(bool all) {
+    tiles_h.clear();
+    chunks_h.clear();
+    const int tx = 1 << log2_tx;
+    for (size_t k = 0; k < tun.size(); ++k) {
+      if (!all && s >= tun[k].steps) continue;
+      const vl::BatchTunnel& T = tun[k];
+      for (int y0 = 0; y0 < T.ny; y0 += ty)
+        for (int x0 = 0; x0 < T.nx; x0 += tx) tiles_h.push_back(make_int4((int)k, y0, x0, 0));
+      for (int c = 0; c < T.nchunks; ++c) chunks_h.push_back(chunks_all[chunk_first[k] + c]);
+    }
+    if (tiles_h.size() > tiles_cap) {
+      if (d_tiles) cudaFree(d_tiles);
+      d_tiles = nullptr;
+      tiles_cap = tiles_h.size();
+      VB_CUDA(cudaMalloc(&d_tiles, tiles_cap * sizeof(int4)));
+    }
+    VB_CUDA(cudaMemcpyAsync(d_tiles, tiles_h.data(), tiles_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+    VB_CUDA(cudaMemcpyAsync(d_chunks, chunks_h.data(), chunks_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+    VB_CUDA(cudaStreamSynchronize(stream));
+    ntiles = (int)tiles_h.size();
+    nchunks = (int)chunks_h.size();
+    P.tiles = d_tiles;
+    P.chunks = d_chunks;
+    P.log2_tx = log2_tx;
+    P.ty = ty;
+    if (gexec) {
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    return VL_OK;
+  }
+
+  cudaError_t enqueue_step() {
+    cudaError_t e;
+    cudaStream_t ls = schedule == 0 ? aux : stream;
+    if (schedule == 0) {
+      if ((e = cudaEventRecord(ev_fork, stream)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(aux, ev_fork, 0)) != cudaSuccess) return e;
+    }
+    if (schedule == 2) {
+      if ((e = L->batch_step(P, ntiles, nchunks, 2, a(), b(), stream)) != cudaSuccess) return e;
+      return L->batch_step(P, ntiles, nchunks, 1, a(), b(), stream);
+    }
+    if ((e = L->batch_step(P, ntiles, nchunks, 1, a(), b(), ls)) != cudaSuccess) return e;
+    if (schedule == 0 && (e = cudaEventRecord(ev_join, aux)) != cudaSuccess) return e;
+    if ((e = L->batch_step(P, ntiles, nchunks, 2, a(), b(), stream)) != cudaSuccess) return e;
+    if (schedule == 0) return cudaStreamWaitEvent(stream, ev_join, 0);
+    return cudaSuccess;
+  }
+
+  int ensure_graph() {
+    if (gexec) return VL_OK;
+    cudaGraph_t g = nullptr;
+    const uint64_t saved = s;
+    VB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kGraphSteps; ++k) {
+      cudaError_t e = enqueue_step();
+      ++s;
+      if (e != cudaSuccess) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        s = saved;
+        return cuda_fail(e, "batch graph capture");
+      }
+    }
+    s = saved;
+    VB_CUDA(cudaStreamEndCapture(stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "batch graph instantiate");
+    return VL_OK;
+  }
+
+  int run(uint64_t max_steps) {
+    VB_CUDA(cudaSetDevice(device));
+    uint64_t end_all = 0;
+    for (auto& T : tun) end_all = std::max<uint64_t>(end_all, T.steps);
+    const uint64_t stop = max_steps ? std::min<uint64_t>(end_all, s + max_steps) : end_all;
+    VB_CUDA(cudaEventRecord(ev0, stream));
+    while (s < stop) {
+      uint64_t seg_end = stop;
+      for (auto& T : tun)
+        if (T.steps > s) seg_end = std::min<uint64_t>(seg_end, T.steps);
+      int rc = build_lists(false);
+      if (rc) return rc;
+      while (s < seg_end) {
+        if (seg_end - s >= (uint64_t)kGraphSteps && (s & 1) == 0) {
+          rc = ensure_graph();
+          if (rc) return rc;
+          VB_CUDA(cudaGraphLaunch(gexec, stream));
+          s += kGraphSteps;
+          launches += 2 * kGraphSteps;
+        } else {
+          cudaError_t e = enqueue_step();
+          if (e != cudaSuccess) return cuda_fail(e, "batch step");
+          ++s;
+          launches += 2;
+        }
+      }
+    }
+    VB_CUDA(cudaEventRecord(ev1, stream));
+    VB_CUDA(cudaStreamSynchronize(stream));
+    timed = true;
+    return VL_OK;
+  }
+
+  // Times the candidate tile shapes on the current state without advancing it and keeps the
+  // fastest. Shapes: 256 x 1, 128 x 2, 64 x 4, 32 x 8 cells.
+  int autotune(int steps_each, double* ms4) {
+    VB_CUDA(cudaSetDevice(device));
+    const int shapes[4][2] = {{8, 1}, {7, 2}, {6, 4}, {5, 8}};
+    double best = 1e300;
+    int bi = 0;
+    P.dry = 1;
+    for (int c = 0; c < 4; ++c) {
+      log2_tx = shapes[c][0];
+      ty = shapes[c][1];
+      int rc = build_lists(false);
+      if (rc) { P.dry = 0; return rc; }
+      for (int k = 0; k < steps_each + 2; ++k) {
+        if (k == 2) VB_CUDA(cudaEventRecord(ev0, stream));
+        cudaError_t e = enqueue_step();
+        if (e != cudaSuccess) { P.dry = 0; return cuda_fail(e, "batch autotune"); }
+      }
+      VB_CUDA(cudaEventRecord(ev1, stream));
+      VB_CUDA(cudaEventSynchronize(ev1));
+      float ms = 0.f;
+      VB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+      if (ms4) ms4[c] = ms / steps_each;
+      if (ms < best) { best = ms; bi = c; }
+    }
+    P.dry = 0;
+    log2_tx = shapes[bi][0];
+    ty = shapes[bi][1];
+    timed = false;
+    return build_lists(false);
+  }
+};
+
+extern "C" {
+
+vl_batch* vl_batch_new(int precision) {
+  const vl::Launchers* L = nullptr;
+  switch (precision) {
+    case VL_F64: L = &vl::launchers_f64(); break;
+    case VL_F32: L = &vl::launchers_f32(); break;
+    case VL_F16S: L = &vl::launchers_f16s(); break;
+    default: fail(VL_EINVAL, "unknown precision"); return nullptr;
+  }
+  auto b = new vl_batch();
+  b->prec = precision;
+  b->L = L;
+  return b;
+}
+
+void vl_batch_free(vl_batch* b) { delete b; }
+
+int vl_batch_add_channel(vl_batch* b, const vl_channel_spec* sp, uint64_t steps) {
+  std::unique_ptr<vl::Shape> body;
+  if (sp && sp->body) { body = std::move(sp->body->s); delete sp->body; }
+  if (!b || !sp) return fail(VL_EINVAL, "null batch or spec");
+  if (b->built) return fail(VL_EINVAL, "batch already built");
+  if (steps == 0) return fail(VL_EINVAL, "a tunnel needs at least one step");
+  vl::ChannelPlan plan;
+  int rc = vl::plan_channel(sp, std::move(body), plan);
+  if (rc) return rc;
+  if (plan.dom.ngroups != 1) return fail(VL_EINVAL, "batched tunnels need a body with force group 0");
+  b->plans.push_back(std::move(plan));
+  b->steps.push_back(steps);
+  return (int)b->plans.size() - 1;
+}
+
+int vl_batch_build(vl_batch* b) {
+  if (!b) return fail(VL_EINVAL, "null batch");
+  if (b->built) return fail(VL_EINVAL, "batch already built");
+  if (b->plans.empty()) return fail(VL_EINVAL, "empty batch");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(VL_ECUDA, "no CUDA device: vortexlab-b200 has no CPU fallback");
+  }
+  VB_CUDA(cudaGetDevice(&b->device));
+  const size_t nt = b->plans.size();
+  std::vector<uint8_t> flag;
+  std::vector<int32_t> bidx, bfirst, pidx;
+  std::vector<int8_t> pn;
+  std::vector<vl::LinkRecDev> links;
+  std::vector<double> sched;
+  unsigned long long pop = 0, cells = 0, hist = 0;
+  int nchunk = 0;
+  b->tun.resize(nt);
+  b->chunk_first.resize(nt);
+  for (size_t k = 0; k < nt; ++k) {
+    const vl::ChannelPlan& pl = b->plans[k];
+    const vl::CompiledDomain& d = pl.dom;
+    vl::BatchTunnel& T = b->tun[k];
+    std::memset(&T, 0, sizeof T);
+    T.nx = (int)d.nx;
+    T.ny = (int)d.ny;
+    T.ns = (unsigned)((d.n + 63) / 64 * 64);
+    if ((unsigned long long)T.ns * 9ull > 0xFFFFFFFFull) return fail(VL_EINVAL, "tunnel too large");
+    T.coll = d.collision;
+    T.pop_off = pop;
+    pop += 9ull * T.ns;
+    T.cell_off = cells;
+    cells += d.n;
+    T.b_off = (int)bidx.size();
+    T.nb = (int)d.bnode_idx.size();
+    T.p_off = (int)pidx.size();
+    T.np = (int)d.pnode_idx.size();
+    T.nchunks = (T.nb + vl::kBlock - 1) / vl::kBlock;
+    T.chunk_off = nchunk;
+    T.op = d.op;
+    T.om = d.om;
+    T.u_ref = pl.u_ref;
+    T.absorbing = 1;
+    T.sched_off = sched.size();
+    T.sched_len = pl.sched_len;
+    T.steps = b->steps[k];
+    T.hist_off = hist;
+    hist += T.steps;
+    flag.insert(flag.end(), d.flag.begin(), d.flag.end());
+    const int32_t loff = (int32_t)links.size();
+    for (int32_t v : d.bnode_idx) bidx.push_back(v);
+    for (size_t j = 0; j + 1 < d.bnode_first.size(); ++j) bfirst.push_back(d.bnode_first[j] + loff);
+    for (const vl::LinkRec& h : d.links) {
+      vl::LinkRecDev g;
+      g.q = h.q; g.cu6 = h.cu6; g.uw0 = h.uw[0]; g.uw1 = h.uw[1]; g.rho = h.rho;
+      g.behind = h.behind; g.dir = h.dir; g.flags = h.flags; g.vgroup = h.vgroup; g.fgroup = h.fgroup;
+      links.push_back(g);
+    }
+    for (size_t j = 0; j < d.pnode_idx.size(); ++j) {
+      pidx.push_back(d.pnode_idx[j]);
+      pn.push_back(d.pnode_nx[j]);
+      pn.push_back(d.pnode_ny[j]);
+    }
+    sched.insert(sched.end(), pl.sched.begin(), pl.sched.begin() + 2 * pl.sched_len);
+    b->chunk_first[k] = (int)b->chunks_all.size();
+    for (int c = 0; c < T.nchunks; ++c)
+      b->chunks_all.push_back(make_int4((int)k, T.b_off + c * vl::kBlock, std::min(vl::kBlock, T.nb - c * vl::kBlock), nchunk + c));
+    nchunk += T.nchunks;
+  }
+  bfirst.push_back((int32_t)links.size());
+  if (links.size() > 0x7fffffffu || cells > 0xFFFFFFFFull) return fail(VL_EINVAL, "batch too large");
+  const size_t pop_bytes = pop * b->L->elem;
+  VB_CUDA(cudaMalloc(&b->buf[0], pop_bytes));
+  VB_CUDA(cudaMalloc(&b->buf[1], pop_bytes));
+  int rc;
+  if ((rc = upload(&b->d_flag, flag)) || (rc = upload(&b->d_bidx, bidx)) || (rc = upload(&b->d_bfirst, bfirst)) ||
+      (rc = upload(&b->d_links, links)) || (rc = upload(&b->d_pidx, pidx)) || (rc = upload(&b->d_pn, pn)) ||
+      (rc = upload(&b->d_sched, sched)) || (rc = upload(&b->d_tun, b->tun)))
+    return rc;
+  std::vector<vl::BatchState> st(nt);
+  std::memset(st.data(), 0, st.size() * sizeof(vl::BatchState));
+  if ((rc = upload(&b->d_st, st))) return rc;
+  VB_CUDA(cudaMalloc(&b->d_chunks, std::max<size_t>(b->chunks_all.size(), 1) * sizeof(int4)));
+  VB_CUDA(cudaMalloc(&b->d_partials, std::max(nchunk, 1) * 2 * sizeof(double)));
+  VB_CUDA(cudaMalloc(&b->d_hist, std::max<unsigned long long>(hist, 1) * 2 * sizeof(double)));
+  VB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  VB_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+  VB_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  VB_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+  VB_CUDA(cudaEventCreate(&b->ev0));
+  VB_CUDA(cudaEventCreate(&b->ev1));
+  // Start states: uniform rest, or the inflow profile when the tunnel has no ramp
+  // (src/cases/channel.rs:108-110), into both buffers.
+  for (size_t k = 0; k < nt; ++k) {
+    const vl::ChannelPlan& pl = b->plans[k];
+    const vl::BatchTunnel& T = b->tun[k];
+    double* field = nullptr;
+    if (pl.init_profile) {
+      std::vector<double> rho, ux, uy;
+      vl::profile_field(pl, rho, ux, uy);
+      const size_t n = pl.dom.n;
+      VB_CUDA(cudaMalloc(&field, 3 * n * sizeof(double)));
+      VB_CUDA(cudaMemcpy(field, rho.data(), n * 8, cudaMemcpyHostToDevice));
+      VB_CUDA(cudaMemcpy(field + n, ux.data(), n * 8, cudaMemcpyHostToDevice));
+      VB_CUDA(cudaMemcpy(field + 2 * n, uy.data(), n * 8, cudaMemcpyHostToDevice));
+    }
+    const size_t n = pl.dom.n;
+    cudaError_t e = b->L->init((int)n, T.ns, b->d_flag + T.cell_off, field, field ? field + n : nullptr,
+                               field ? field + 2 * n : nullptr, 1.0, 0.0, 0.0, b->tunnel_ptr(b->buf[0], (int)k),
+                               b->tunnel_ptr(b->buf[1], (int)k), b->stream);
+    if (field) {
+      cudaStreamSynchronize(b->stream);
+      cudaFree(field);
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "batch init");
+  }
+  VB_CUDA(cudaStreamSynchronize(b->stream));
+  vl::BatchParams& P = b->P;
+  P.tun = b->d_tun;
+  P.st = b->d_st;
+  P.flag = b->d_flag;
+  P.bnode_idx = b->d_bidx;
+  P.bnode_first = b->d_bfirst;
+  P.links = b->d_links;
+  P.pnode_idx = b->d_pidx;
+  P.pnode_n = b->d_pn;
+  P.sched = b->d_sched;
+  P.partials = b->d_partials;
+  P.hist = b->d_hist;
+  P.sqrt_cs2 = std::sqrt(1.0 / 3.0);
+  P.dry = 0;
+  b->built = true;
+  // The host plans (domains) are no longer needed on the host except their sizes.
+  for (auto& pl : b->plans) {
+    pl.dom.links.clear();
+    pl.dom.links.shrink_to_fit();
+  }
+  return b->build_lists(false);
+}
+
+int vl_batch_size(const vl_batch* b) { return b ? (int)b->plans.size() : VL_EINVAL; }
+
+int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_t* fluid, uint64_t* steps) {
+  if (!b || k < 0 || (size_t)k >= b->plans.size()) return fail(VL_EINVAL, "tunnel index out of range");
+  if (nx) *nx = b->plans[k].dom.nx;
+  if (ny) *ny = b->plans[k].dom.ny;
+  if (fluid) *fluid = b->plans[k].dom.fluid_nodes;
+  if (steps) *steps = b->steps[k];
+  return VL_OK;
+}
+
+int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty) {
+  if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
+  if (log2_tx < 5 || log2_tx > 8 || ty < 1 || (ty << log2_tx) != vl::kBlock)
+    return fail(VL_EINVAL, "tile must be 2^log2_tx x ty = 256 cells with 32 <= 2^log2_tx <= 256");
+  b->log2_tx = log2_tx;
+  b->ty = ty;
+  return b->build_lists(false);
+}
+
+int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty) {
+  if (!b) return fail(VL_EINVAL, "null batch");
+  if (log2_tx) *log2_tx = b->log2_tx;
+  if (ty) *ty = b->ty;
+  return VL_OK;
+}
+
+int vl_batch_set_schedule(vl_batch* b, int schedule) {
+  if (!b || schedule < 0 || schedule > 2) return fail(VL_EINVAL, "schedule must be 0, 1 or 2");
+  b->schedule = schedule;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return VL_OK;
+}
+
+int vl_batch_autotune(vl_batch* b, int steps_each, double* ms4) {
+  if (!b || !b->built || steps_each < 1) return fail(VL_EINVAL, "autotune: bad arguments");
+  return b->autotune(steps_each, ms4);
+}
+
+int vl_batch_run(vl_batch* b, uint64_t max_steps) {
+  if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
+  return b->run(max_steps);
+}
+
+int vl_batch_last_run_ms(vl_batch* b, float* ms) {
+  if (!b || !ms || !b->timed) return fail(VL_EINVAL, "no run timed yet");
+  VB_CUDA(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+  return VL_OK;
+}
+
+int vl_batch_global_step(const vl_batch* b, uint64_t* s) {
+  if (!b || !s) return fail(VL_EINVAL, "null argument");
+  *s = b->s;
+  return VL_OK;
+}
+
+int vl_batch_launch_count(const vl_batch* b, uint64_t* out) {
+  if (!b || !out) return fail(VL_EINVAL, "null argument");
+  *out = b->launches;
+  return VL_OK;
+}
+
+static int pull_state(vl_batch* b, int k, vl::BatchState* st) {
+  VB_CUDA(cudaMemcpyAsync(st, b->d_st + k, sizeof *st, cudaMemcpyDeviceToHost, b->stream));
+  VB_CUDA(cudaStreamSynchronize(b->stream));
+  return VL_OK;
+}
+
+int vl_batch_status(vl_batch* b, int k, uint64_t* t, int* nonfinite, double* force2) {
+  if (!b || !b->built || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "tunnel index out of range");
+  vl::BatchState st;
+  int rc = pull_state(b, k, &st);
+  if (rc) return rc;
+  if (t) *t = st.t;
+  if (nonfinite) *nonfinite = st.nonfinite;
+  if (force2) { force2[0] = st.force[0]; force2[1] = st.force[1]; }
+  return VL_OK;
+}
+
+int vl_batch_force_history(vl_batch* b, int k, double* out, uint64_t* count) {
+  if (!b || !b->built || !count || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  vl::BatchState st;
+  int rc = pull_state(b, k, &st);
+  if (rc) return rc;
+  const uint64_t have = std::min<uint64_t>(st.t, b->tun[k].steps);
+  if (out && have)
+    VB_CUDA(cudaMemcpy(out, b->d_hist + 2 * b->tun[k].hist_off, have * 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  *count = have;
+  return VL_OK;
+}
+
+int vl_batch_download(vl_batch* b, int k, double* out) {
+  if (!b || !b->built || !out || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  vl::BatchState st;
+  int rc = pull_state(b, k, &st);
+  if (rc) return rc;
+  const size_t n = b->plans[k].dom.n;
+  const vl::BatchTunnel& T = b->tun[k];
+  double* tmp = nullptr;
+  VB_CUDA(cudaMalloc(&tmp, 9 * n * sizeof(double)));
+  cudaError_t e = b->L->to_f64((int)n, T.ns, b->tunnel_ptr(b->buf[st.t & 1], k), tmp, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, 9 * n * 8, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(e, "batch download");
+  return VL_OK;
+}
+
+int vl_batch_flags(vl_batch* b, int k, uint8_t* out) {
+  if (!b || !out || k < 0 || (size_t)k >= b->plans.size()) return fail(VL_EINVAL, "bad arguments");
+  std::memcpy(out, b->plans[k].dom.flag.data(), b->plans[k].dom.n);
+  return VL_OK;
+}
+
+int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out) {
+  if (!b || !out || k < 0 || (size_t)k >= b->plans.size()) return fail(VL_EINVAL, "bad arguments");
+  const size_t n = b->plans[k].dom.n;
+  std::vector<double> f(9 * n);
+  int rc = vl_batch_download(b, k, f.data());
+  if (rc) return rc;
+  const std::vector<uint8_t>& flag = b->plans[k].dom.flag;
+  uint64_t h = 0xcbf29ce484222325ull;
+  for (size_t idx = 0; idx < n; ++idx) {
+    if (flag[idx] == 2) continue;
+    for (int i = 0; i < 9; ++i) {
+      uint64_t bits;
+      std::memcpy(&bits, &f[(size_t)i * n + idx], 8);
+      for (int q = 0; q < 8; ++q) {
+        h ^= (bits >> (8 * q)) & 0xffu;
+        h *= 0x100000001b3ull;
+      }
+    }
+  }
+  *out = h;
+  return VL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,172 @@
+// Batched step kernels: many tunnels (channels) of uneven sizes advanced together, one launch per
+// kernel per step over the work of every active tunnel.
+//
+// All tunnels live in one arena: each tunnel's nine population planes are contiguous at its own
+// offset in the two population buffers, its cells at its own offset in the flag array, and its
+// boundary nodes, links and outlet nodes are concatenated into shared tables (link indices are
+// global; cell indices stay local to the tunnel). A bulk work item is a tile of a tunnel (2^log2_tx
+// cells x ty rows); a link work item is a chunk of up to kBlock boundary nodes of a tunnel. The
+// last chunk of a tunnel to finish a step runs that tunnel's epilogue (force reduction in the same
+// fixed order as a single sim, force record, t + 1). The per-node arithmetic is the single-sim
+// code (pull, link_node, collide), so a tunnel in a batch is bit-identical to the same tunnel run
+// alone.
+#pragma once
+
+#include "vl_device.cuh"
+
+namespace vl {
+
+struct BatchTunnel {
+  int nx, ny;
+  unsigned ns;                  // population plane stride of this tunnel
+  int coll;                     // COLL_BGK or COLL_TRT
+  unsigned long long pop_off;   // element offset of the tunnel's plane 0 in each population buffer
+  unsigned long long cell_off;  // offset of the tunnel's cells in the flag array
+  int b_off, nb;                // boundary nodes (global index of the first, count)
+  int p_off, np;                // outlet nodes
+  int chunk_off, nchunks;       // link chunks
+  double op, om;
+  double u_ref;
+  int absorbing;
+  int pad;
+  unsigned long long sched_off, sched_len;
+  unsigned long long steps;     // steps to run
+  unsigned long long hist_off;  // first force record (2 doubles per step)
+};
+
+struct BatchState {
+  unsigned long long t;
+  unsigned long long nonfinite_t;
+  unsigned int arrive;
+  int nonfinite;
+  double drho;
+  double force[2];
+};
+
+struct BatchParams {
+  const BatchTunnel* tun;
+  BatchState* st;
+  const int4* tiles;            // (tunnel, y0, x0, -)
+  int log2_tx, ty;
+  const int4* chunks;           // (tunnel, first boundary node, count, global chunk index)
+  const uint8_t* flag;
+  const int32_t* bnode_idx;     // cell index local to the tunnel
+  const int32_t* bnode_first;   // global link index; total_nb + 1 entries
+  const void* links;
+  const int32_t* pnode_idx;     // local cell index
+  const int8_t* pnode_n;
+  const double* sched;          // per tunnel: 2 doubles per step
+  double* partials;             // 2 doubles per chunk
+  double* hist;                 // 2 doubles per recorded step
+  double sqrt_cs2;
+  int dry;                      // timing runs: commit nothing
+};
+
+// Controls of a tunnel at its step t (src/cases/channel.rs:118-130).
+__device__ __forceinline__ void tunnel_controls(const BatchParams& p, const BatchTunnel& T, unsigned long long t,
+                                                double* vs, double& target) {
+  double v1 = 1.0, v2 = 0.0;
+  if (t < T.sched_len) {
+    v1 = p.sched[T.sched_off + 2 * t];
+    v2 = p.sched[T.sched_off + 2 * t + 1];
+  }
+  vs[0] = 1.0;
+  vs[1] = v1;
+  vs[2] = v2;
+  vs[3] = 1.0;
+  target = T.u_ref * v1;
+}
+
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ BatchParams p, const S* __restrict__ A,
+                                                       S* __restrict__ B) {
+  using R = typename Store<S>::R;
+  // Only tunnels that are active for the whole launch are in the tile list (the host rebuilds it
+  // when a tunnel finishes), so the tile never checks the tunnel's t, which the link kernel's
+  // epilogue may advance concurrently.
+  const int4 td = __ldg(p.tiles + blockIdx.x);
+  const BatchTunnel& T = p.tun[td.x];
+  const int nx = T.nx, ny = T.ny;
+  const int x = td.z + (int)(threadIdx.x & ((1u << p.log2_tx) - 1u));
+  const int y = td.y + (int)(threadIdx.x >> p.log2_tx);
+  if (x >= nx || y >= ny) return;
+  const S* a = A + T.pop_off;
+  S* b = B + T.pop_off;
+  const unsigned idx = (unsigned)(y * nx + x);
+  const uint8_t fl = __ldg(p.flag + T.cell_off + idx);
+  R f[9];
+  pull(a, T.ns, nx, ny, x, y, f);
+  if (T.coll == COLL_BGK)
+    collide_bgk(f, (R)T.op);
+  else
+    collide_trt(f, (R)T.op, (R)T.om);
+  if (fl != 0) return;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * T.ns + idx, i, f[i]);
+}
+
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ BatchParams p, const S* __restrict__ A,
+                                                        S* __restrict__ B) {
+  using R = typename Store<S>::R;
+  __shared__ double s_un[kBlock];
+  __shared__ double s_acc[2][kBlock];
+  __shared__ double red[kBlock];
+  __shared__ int last;
+  const int tid = threadIdx.x;
+  const int4 cd = __ldg(p.chunks + blockIdx.x);
+  const BatchTunnel& T = p.tun[cd.x];
+  BatchState* st = &p.st[cd.x];
+  const unsigned long long t = st->t;
+  if (t >= T.steps) return;
+  const S* a = A + T.pop_off;
+  S* b = B + T.pop_off;
+  double vs[4], target;
+  tunnel_controls(p, T, t, vs, target);
+  const double drho = (T.absorbing && T.np > 0)
+                          ? outlet_offset(a, T.ns, p.pnode_idx + T.p_off, p.pnode_n + 2 * T.p_off, T.np, 0.0, 0.0,
+                                          target, p.sqrt_cs2, s_un)
+                          : 0.0;
+  if (cd.w == T.chunk_off && tid == 0 && !p.dry) st->drho = drho;
+  s_acc[0][tid] = 0.0;
+  s_acc[1][tid] = 0.0;
+  if (tid < cd.z) {
+    const int g = cd.y + tid;
+    const int idx = __ldg(p.bnode_idx + g);
+    R f[9];
+    link_node<S>(a, T.ns, T.nx, T.ny, idx, __ldg(p.bnode_first + g), __ldg(p.bnode_first + g + 1),
+                 (const LinkRecDev*)p.links, vs, drho, T.coll, T.op, T.om, 0.0, 0.0, p.sqrt_cs2, &s_acc[0][tid], f);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * T.ns + idx, i, f[i]);
+  }
+  __syncthreads();
+  block_force_partial(s_acc, 2, p.partials + 2 * (size_t)cd.w);
+  // The last chunk of this tunnel reduces the tunnel's partials and advances its step.
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    last = atomicAdd(&st->arrive, 1u) == (unsigned)(T.nchunks - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double fx = sum_partials(p.partials + 2 * (size_t)T.chunk_off, T.nchunks, 2, red);
+  const double fy = sum_partials(p.partials + 2 * (size_t)T.chunk_off + 1, T.nchunks, 2, red);
+  if (tid == 0) {
+    if (!p.dry) {
+      st->force[0] = fx;
+      st->force[1] = fy;
+      if (!(isfinite(fx) && isfinite(fy)) && !st->nonfinite) {
+        st->nonfinite = 1;
+        st->nonfinite_t = t;
+      }
+      p.hist[2 * (T.hist_off + t)] = fx;
+      p.hist[2 * (T.hist_off + t) + 1] = fy;
+      st->t = t + 1;
+    }
+    st->arrive = 0;
+    __threadfence();
+  }
+}
+
+}  // namespace vl

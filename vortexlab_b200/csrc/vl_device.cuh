@@ -213,6 +213,23 @@ __device__ void record_probe(const StepParams& p, const S* __restrict__ a, long 
   __syncthreads();
 }
 
+// Block-wide sum of `count` values spaced `stride` apart: thread t adds values t, t + kBlock, ...
+// in order, then a fixed shared-memory tree. The result is valid in thread 0. Every thread calls it.
+__device__ __forceinline__ double sum_partials(const double* v, int count, int stride, double* red) {
+  const int tid = threadIdx.x;
+  double acc = 0.0;
+  for (int k = tid; k < count; k += kBlock) acc += __ldcg(v + (size_t)k * stride);
+  red[tid] = acc;
+  __syncthreads();
+  for (int s = kBlock / 2; s > 0; s >>= 1) {
+    if (tid < s) red[tid] += red[tid + s];
+    __syncthreads();
+  }
+  const double out = red[0];
+  __syncthreads();
+  return out;
+}
+
 // Runs in the last link block to finish a step: reduces the force partials in a fixed order,
 // writes the step record, evaluates the pressure probe of the previous step (whose result is the
 // current `a`), advances the controls and t.
@@ -223,21 +240,11 @@ __device__ void step_epilogue(const StepParams& p, const S* __restrict__ a) {
   const int tid = threadIdx.x;
   Ctl* c = p.ctl;
   const int ncomp = 2 * p.ngroups;
-  // force: each component summed over the link-block partials with a fixed stride pattern, then
-  // a fixed shared-memory tree (one component at a time, to keep shared memory small).
   for (int k = 0; k < ncomp; ++k) {
-    double acc = 0.0;
-    for (int blk = tid; blk < p.nlink; blk += kBlock)
-      acc += __ldcg(p.partials + (size_t)blk * (2 * kMaxGroups) + k);
-    red[tid] = acc;
-    __syncthreads();
-    for (int s = kBlock / 2; s > 0; s >>= 1) {
-      if (tid < s) red[tid] += red[tid + s];
-      __syncthreads();
-    }
-    if (tid == 0) res[k] = red[0];
-    __syncthreads();
+    const double v = sum_partials(p.partials + k, p.nlink, 2 * kMaxGroups, red);
+    if (tid == 0) res[k] = v;
   }
+  __syncthreads();
   const unsigned long long t = c->t;
   const bool commit = !c->dry;
   if (commit) record_probe<S>(p, a, (long long)t - 1);
@@ -371,148 +378,166 @@ __device__ __forceinline__ LinkView load_link(const LinkRecDev* links, int l) {
   return L;
 }
 
+// Outlet density offset (src/sim.rs:444-455): the velocity of every non-radiating pressure node
+// from its own populations in `a`, summed sequentially in pnode order. Block-wide; every thread
+// calls it and receives the result.
+template <class S>
+__device__ double outlet_offset(const S* __restrict__ a, unsigned ns, const int32_t* __restrict__ pnode_idx,
+                                const int8_t* __restrict__ pnode_n, int np, double gx, double gy, double target,
+                                double sqrt_cs2, double* s_un) {
+  __shared__ double s_drho;
+  const int tid = threadIdx.x;
+  double sum = 0.0;
+  for (int base = 0; base < np; base += kBlock) {
+    const int k = base + tid;
+    if (k < np) {
+      const int idx = __ldg(pnode_idx + k);
+      double f[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
+      double rho, jx, jy;
+      moments(f, rho, jx, jy);
+      const double ux = jx / rho - 0.5 * gx, uy = jy / rho - 0.5 * gy;
+      s_un[tid] = (double)pnode_n[2 * k] * ux + (double)pnode_n[2 * k + 1] * uy;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      const int m = min(kBlock, np - base);
+      for (int q = 0; q < m; ++q) sum += s_un[q];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) s_drho = (sum / (double)np - target) / sqrt_cs2;
+  __syncthreads();
+  return s_drho;
+}
+
+// The link pass for one boundary node (src/sim.rs:456-503): the incoming populations (pulled
+// from the neighbours), each population that would come out of the boundary replaced by the rule
+// of its link, the momentum exchanged with each force group added to `acc` (component c at
+// acc[c * kBlock]), then the collision. `f` returns the post-collision populations.
+template <class S>
+__device__ __forceinline__ void link_node(const S* __restrict__ a, unsigned ns, int nx, int ny, int idx, int first,
+                                          int last, const LinkRecDev* __restrict__ links, const double* vs,
+                                          double drho, int ck, double op_, double om_, double gx_, double gy_,
+                                          double sqrt_cs2, double* acc, typename Store<S>::R* f) {
+  using R = typename Store<S>::R;
+  const R op = (R)op_, om = (R)om_, gx = (R)gx_, gy = (R)gy_;
+  const int y = idx / nx, x = idx - y * nx;
+  // The incoming populations and the node's own post-collision populations: every per-link read
+  // of the reference's link pass other than the node behind the link (a[j][idx], a[i][idx], the
+  // node velocity) is one of the own values, so the link loop touches memory only for its record
+  // and that one node.
+  R own[9];
+  pull(a, ns, nx, ny, x, y, f);
+#pragma unroll
+  for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
+  bool have_u = false;
+  R ux = R(0), uy = R(0);
+  for (int l = first; l < last; ++l) {
+    const LinkView L = load_link(links, l);
+    const int j = L.dir;
+    const int i = opp_of(j);
+    const R out = pick(own, j);
+    const R scale = (R)vs[L.vgroup];
+    R back;
+    if (!(L.flags & 1)) {
+      // Wall: interpolated bounce-back with the moving-wall term (src/sim.rs:467-479).
+      const R corr = (R)L.cu6 * scale;
+      const R q = (R)L.q;
+      if (q >= R(0.5)) {
+        const R kq = R(0.5) / q;
+        back = kq * (out - corr) + (R(1.0) - kq) * pick(own, i);
+      } else if (L.behind >= 0) {
+        back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * Store<S>::ld(a + (unsigned)j * ns + (unsigned)L.behind, j) - corr;
+      } else {
+        back = out - corr;
+      }
+    } else {
+      // Open boundary: anti-bounce-back around the equilibrium of the boundary density
+      // (src/sim.rs:480-488), with the node's own velocity.
+      if (!have_u) {
+        R rho, jx, jy;
+        moments(own, rho, jx, jy);
+        ux = jx / rho - R(0.5) * gx;
+        uy = jy / rho - R(0.5) * gy;
+        have_u = true;
+      }
+      const R cu = R(3.0) * ((R)cx_of(j) * ux + (R)cy_of(j) * uy);
+      R rho_w;
+      if (L.flags & 2) {
+        const R nxv = (R)((int)((L.flags >> 2) & 3) - 1), nyv = (R)((int)((L.flags >> 4) & 3) - 1);
+        rho_w = (R)L.rho + (nxv * ux + nyv * uy) / (R)sqrt_cs2;
+      } else {
+        rho_w = (R)L.rho + (R)drho;
+      }
+      back = -out + R(2.0) * (R)w_of(j) * rho_w * (R(1.0) + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy));
+    }
+    set_dir(f, i, back);
+    if (L.fgroup >= 0) {
+      // Galilean-invariant momentum exchange (src/sim.rs:490-495), accumulated in FP64.
+      const double o = (double)out, bk = (double)back;
+      const double wux = L.uw0 * (double)scale, wuy = L.uw1 * (double)scale;
+      acc[(2 * L.fgroup) * kBlock] += (double)cx_of(j) * (o + bk) - wux * (o - bk);
+      acc[(2 * L.fgroup + 1) * kBlock] += (double)cy_of(j) * (o + bk) - wuy * (o - bk);
+    }
+  }
+  if (ck == 2)
+    collide_forced(f, op, om, gx, gy);
+  else if (ck == 0)
+    collide_bgk(f, op);
+  else
+    collide_trt(f, op, om);
+}
+
+// Block partial of the first `ncomp` force components: fixed shuffle tree within each warp, then
+// the warps in order. Written by threads 0..ncomp-1 to out[c]. Every thread calls it.
+__device__ __forceinline__ void block_force_partial(const double (*s_acc)[kBlock], int ncomp, double* out) {
+  __shared__ double s_red[2 * kMaxGroups][kBlock / 32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c = 0; c < ncomp; ++c) {
+    double v = s_acc[c][tid];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+    if (lane == 0) s_red[c][warp] = v;
+  }
+  __syncthreads();
+  if (tid < ncomp) {
+    double v = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) v += s_red[tid][w];
+    out[tid] = v;
+  }
+}
+
 #ifndef VL_LINK_MIN_BLOCKS
 #define VL_LINK_MIN_BLOCKS 1
 #endif
 template <class S, int CK>
 __global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links(const __grid_constant__ StepParams p,
-                                                  const S* __restrict__ a, S* __restrict__ b) {
+                                                                    const S* __restrict__ a, S* __restrict__ b) {
   using R = typename Store<S>::R;
   __shared__ double s_un[kBlock];
-  __shared__ double s_drho;
   __shared__ double s_acc[2 * kMaxGroups][kBlock];
-  __shared__ double s_red[2 * kMaxGroups][kBlock / 32];
   const int tid = threadIdx.x;
-  const int nx = p.nx, ny = p.ny;
-  const unsigned ns = p.ns;
   const Controls ctl = read_controls(p.ctl);
-  const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
-
-  // Outlet density offset (src/sim.rs:444-455): velocity of every non-radiating pressure node
-  // from its own populations in `a`, summed sequentially in pnode order.
-  double drho = 0.0;
-  if (ctl.has_target && p.np > 0) {
-    double sum = 0.0;
-    for (int base = 0; base < p.np; base += kBlock) {
-      const int k = base + tid;
-      if (k < p.np) {
-        const int idx = __ldg(p.pnode_idx + k);
-        double f[9];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) f[i] = (double)Store<S>::ld(a + (size_t)i * ns + idx, i);
-        double rho, jx, jy;
-        moments(f, rho, jx, jy);
-        const double ux = jx / rho - 0.5 * p.gx, uy = jy / rho - 0.5 * p.gy;
-        s_un[tid] = (double)p.pnode_n[2 * k] * ux + (double)p.pnode_n[2 * k + 1] * uy;
-      }
-      __syncthreads();
-      if (tid == 0) {
-        const int m = min(kBlock, p.np - base);
-        for (int q = 0; q < m; ++q) sum += s_un[q];
-      }
-      __syncthreads();
-    }
-    if (tid == 0) s_drho = (sum / (double)p.np - ctl.target) / p.sqrt_cs2;
-    __syncthreads();
-    drho = s_drho;
-  }
+  const double drho = (ctl.has_target && p.np > 0)
+                          ? outlet_offset(a, p.ns, p.pnode_idx, p.pnode_n, p.np, p.gx, p.gy, ctl.target, p.sqrt_cs2, s_un)
+                          : 0.0;
   if (blockIdx.x == 0 && tid == 0 && !p.ctl->dry) p.ctl->drho = drho;
-
-  const bool forces = p.ngroups > 0;
-  if (forces) {
-#pragma unroll
-    for (int k = 0; k < 2 * kMaxGroups; ++k) s_acc[k][tid] = 0.0;
-  }
-
-  const LinkRecDev* links = (const LinkRecDev*)p.links;
+  const int ncomp = 2 * p.ngroups;
+  for (int c = 0; c < ncomp; ++c) s_acc[c][tid] = 0.0;
   const int k = blockIdx.x * kBlock + tid;
   if (k < p.nb) {
     const int idx = __ldg(p.bnode_idx + k);
-    const int first = __ldg(p.bnode_first + k), last = __ldg(p.bnode_first + k + 1);
-    const int y = idx / nx, x = idx - y * nx;
-    // The incoming populations (pulled from the neighbours) and the node's own post-collision
-    // populations: every per-link read of the reference's link pass other than the node behind
-    // the link (a[j][idx], a[i][idx], the node velocity) is one of the own values, so the link
-    // loop below touches memory only for its record and that one node.
-    R f[9], own[9];
-    pull(a, ns, nx, ny, x, y, f);
+    R f[9];
+    link_node<S>(a, p.ns, p.nx, p.ny, idx, __ldg(p.bnode_first + k), __ldg(p.bnode_first + k + 1),
+                 (const LinkRecDev*)p.links, ctl.vs, drho, CK, p.op, p.om, p.gx, p.gy, p.sqrt_cs2, &s_acc[0][tid], f);
 #pragma unroll
-    for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
-    bool have_u = false;
-    R ux = R(0), uy = R(0);
-    for (int l = first; l < last; ++l) {
-      const LinkView L = load_link(links, l);
-      const int j = L.dir;
-      const int i = opp_of(j);
-      const R out = pick(own, j);
-      const R scale = (R)ctl.vs[L.vgroup];
-      R back;
-      if (!(L.flags & 1)) {
-        // Wall: interpolated bounce-back with the moving-wall term (src/sim.rs:467-479).
-        const R corr = (R)L.cu6 * scale;
-        const R q = (R)L.q;
-        if (q >= R(0.5)) {
-          const R kq = R(0.5) / q;
-          back = kq * (out - corr) + (R(1.0) - kq) * pick(own, i);
-        } else if (L.behind >= 0) {
-          back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * Store<S>::ld(a + (unsigned)j * ns + (unsigned)L.behind, j) - corr;
-        } else {
-          back = out - corr;
-        }
-      } else {
-        // Open boundary: anti-bounce-back around the equilibrium of the boundary density
-        // (src/sim.rs:480-488), with the node's own velocity.
-        if (!have_u) {
-          R rho, jx, jy;
-          moments(own, rho, jx, jy);
-          ux = jx / rho - R(0.5) * gx;
-          uy = jy / rho - R(0.5) * gy;
-          have_u = true;
-        }
-        const R cu = R(3.0) * ((R)cx_of(j) * ux + (R)cy_of(j) * uy);
-        R rho_w;
-        if (L.flags & 2) {
-          const R nxv = (R)((int)((L.flags >> 2) & 3) - 1), nyv = (R)((int)((L.flags >> 4) & 3) - 1);
-          rho_w = (R)L.rho + (nxv * ux + nyv * uy) / (R)p.sqrt_cs2;
-        } else {
-          rho_w = (R)L.rho + (R)drho;
-        }
-        back = -out + R(2.0) * (R)w_of(j) * rho_w * (R(1.0) + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy));
-      }
-      set_dir(f, i, back);
-      if (L.fgroup >= 0) {
-        // Galilean-invariant momentum exchange (src/sim.rs:490-495), accumulated in FP64.
-        const double o = (double)out, bk = (double)back;
-        const double wux = L.uw0 * (double)scale, wuy = L.uw1 * (double)scale;
-        s_acc[2 * L.fgroup][tid] += (double)cx_of(j) * (o + bk) - wux * (o - bk);
-        s_acc[2 * L.fgroup + 1][tid] += (double)cy_of(j) * (o + bk) - wuy * (o - bk);
-      }
-    }
-    if (CK == 2)
-      collide_forced(f, op, om, gx, gy);
-    else if (CK == 0)
-      collide_bgk(f, op);
-    else
-      collide_trt(f, op, om);
-#pragma unroll
-    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * ns + idx, i, f[i]);
+    for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * p.ns + idx, i, f[i]);
   }
-
-  // Block partial of the force: fixed shuffle tree within each warp, then fixed order over warps.
-  if (forces) {
-    const int lane = tid & 31, warp = tid >> 5;
-    for (int c = 0; c < 2 * p.ngroups; ++c) {
-      double v = s_acc[c][tid];
-#pragma unroll
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) s_red[c][warp] = v;
-    }
+  if (ncomp > 0) {
     __syncthreads();
-    if (tid < 2 * p.ngroups) {
-      double v = 0.0;
-      for (int w = 0; w < kBlock / 32; ++w) v += s_red[tid][w];
-      p.partials[(size_t)blockIdx.x * (2 * kMaxGroups) + tid] = v;
-    }
+    block_force_partial(s_acc, ncomp, p.partials + (size_t)blockIdx.x * (2 * kMaxGroups));
   }
   arrive<S>(p, a);
 }

@@ -198,6 +198,17 @@ struct CompiledDomain {
 // violation (tau <= 1/2, fluid on a non-periodic edge, vgroup out of range, too many groups).
 bool compile_domain(const DomainSpec& spec, CompiledDomain& out, std::string& err);
 
+// ------------------------------------------------------------------ channel plan
+// Host decisions of Channel::new / Channel::step (src/cases/channel.rs:71-130).
+struct ChannelPlan {
+  CompiledDomain dom;
+  double u_ref = 0.0;
+  bool init_profile = false;        // ramp_steps == 0: start from the inflow profile
+  WallVelocity profile;
+  uint64_t sched_len = 0;           // steps with a non-constant control
+  std::vector<double> sched;        // per step: inlet ramp, body kick
+};
+
 // ------------------------------------------------------------------ signal (src/signal.rs)
 void fft_inplace(double* re, double* im, size_t n);
 double series_mean(const double* x, size_t n);

@@ -10,6 +10,7 @@
 namespace vl {
 
 struct StepParams;
+struct BatchParams;
 
 struct Launchers {
   size_t elem;  // bytes per stored population value
@@ -26,6 +27,9 @@ struct Launchers {
   cudaError_t (*gather)(int m, unsigned ns, const int32_t* cells, const void* a, double* out, cudaStream_t s);
   // Records the pressure probe of the last step of a batch (one block).
   cudaError_t (*probe)(const StepParams& p, const void* a, cudaStream_t s);
+  // One step of a batch of tunnels: which = 1 link kernel, 2 bulk kernel, 3 both.
+  cudaError_t (*batch_step)(const BatchParams& p, int ntiles, int nchunks, int which, const void* a, void* b,
+                            cudaStream_t s);
 };
 
 // Records a failure for vl_last_error / vl_last_status (thread-local) and returns `code`.

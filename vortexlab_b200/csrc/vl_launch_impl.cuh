@@ -1,6 +1,7 @@
 // Launcher bodies shared by the per-precision translation units.
 #pragma once
 
+#include "vl_batch.cuh"
 #include "vl_device.cuh"
 #include "vl_launch.hpp"
 
@@ -61,8 +62,14 @@ struct LaunchImpl {
     k_probe<S><<<1, kBlock, 0, s>>>(p, (const S*)a);
     return cudaGetLastError();
   }
+  static cudaError_t batch_step(const BatchParams& p, int ntiles, int nchunks, int which, const void* a, void* b,
+                                cudaStream_t s) {
+    if ((which & 1) && nchunks > 0) k_batch_links<S><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+    if ((which & 2) && ntiles > 0) k_batch_bulk<S><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+    return cudaGetLastError();
+  }
   static const Launchers& table() {
-    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &probe};
+    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &probe, &batch_step};
     return t;
   }
 };

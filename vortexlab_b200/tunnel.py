@@ -35,15 +35,19 @@ class Tunnel:
     def steps_per_unit(self) -> float:
         return float(self.d) / self.u
 
-    def build(self, body) -> Channel:
-        """src/cases/tunnel.rs:52-67: 5-unit inflow ramp, then a 2-unit twist of the body."""
+    def spec(self, body) -> Spec:
+        """The channel of src/cases/tunnel.rs:52-67: 5-unit inflow ramp, then a 2-unit twist of the
+        body."""
         nx, ny = self.grid()
         cx, cy = self.centre()
         unit = self.steps_per_unit()
-        spec = Spec(nx=nx, ny=ny, inflow=Inflow.UniformOpen(self.u) if self.open_sides else Inflow.Uniform(self.u),
+        return Spec(nx=nx, ny=ny, inflow=Inflow.UniformOpen(self.u) if self.open_sides else Inflow.Uniform(self.u),
                     nu=self.u * self.d / self.re, collision=self.collision, body=body, ramp_steps=int(5.0 * unit),
                     kick=Kick(cx, cy, 0.4 * self.u / self.d, int(5.0 * unit), int(2.0 * unit)))
-        return Channel(spec, precision=self.precision)
+
+    def build(self, body) -> Channel:
+        """src/cases/tunnel.rs:52-67."""
+        return Channel(self.spec(body), precision=self.precision)
 
     def run(self, ch: Channel, units: float) -> Series:
         """src/cases/tunnel.rs:71-92 (force coefficients every step, recorded on the device)."""
