@@ -287,6 +287,17 @@ int vl_batch_download(vl_batch* b, int k, double* out);
 int vl_batch_flags(vl_batch* b, int k, uint8_t* out);
 int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
 
+/* ================================================================ learned warm start: kernels
+ * No reference counterpart. Device-pointer kernels of the warm-start network (a convolutional
+ * network trained on solver-generated wakes); the caller owns every buffer.
+ * vl_nn_gemm_bf16: out[m, n] = epilogue(sum_k a[m, k] * b[n, k]) on the tcgen05 tensor cores,
+ * BF16 inputs (row-major, K contiguous, leading dimensions lda / ldb multiples of 8), FP32
+ * accumulation. flags: 1 accumulate into FP32 out, 2 add bias[n], 4 ReLU, 8 store BF16.
+ * bn: tile width 32, 64, 128 or 256. err (device int, may be NULL) becomes nonzero if a tile
+ * timed out waiting for its data. Asynchronous on `stream`. */
+int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N, int K, void* out, int ldc,
+                    const float* bias, int flags, int bn, int* err, void* stream);
+
 /* ================================================================ signal: src/signal.rs */
 int vl_fft(double* re, double* im, size_t n);                              /* :6-44 */
 double vl_mean(const double* x, size_t n);                                 /* :61-63 */

@@ -1,0 +1,59 @@
+"""The tcgen05 BF16 GEMM (C = A B^T, FP32 accumulation in tensor memory) against an FP64 product
+of the same BF16 inputs, on shapes that are not tile multiples (TMA zero-fills the edges), for
+every tile width and epilogue."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+EPI_ACCUM, EPI_BIAS, EPI_RELU, EPI_BF16 = 1, 2, 4, 8
+
+
+def _gemm(V, a, b, out, flags=0, bias=None, bn=128):
+    import torch
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    M, K = a.shape
+    N = b.shape[0]
+    rc = V.lib.vl_nn_gemm_bf16(C.c_void_p(a.data_ptr()), K, C.c_void_p(b.data_ptr()), K, M, N, K,
+                               C.c_void_p(out.data_ptr()), out.shape[1],
+                               C.cast(C.c_void_p(bias.data_ptr() if bias is not None else 0), C.POINTER(C.c_float)),
+                               flags, bn, C.cast(C.c_void_p(err.data_ptr()), C.POINTER(C.c_int)), None)
+    assert rc == 0, V._lib.last_error()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+
+
+@pytest.mark.parametrize("M,N,K,bn", [(128, 32, 64, 32), (256, 64, 128, 64), (300, 200, 1000, 128),
+                                      (1000, 256, 576, 256), (130, 96, 72, 32), (4096, 128, 288, 128)])
+def test_gemm_matches_fp64(gpu, M, N, K, bn):
+    V = gpu
+    import torch
+    g = torch.Generator().manual_seed(M * 7 + N * 3 + K)
+    a = torch.randn(M, K, generator=g).bfloat16()
+    b = torch.randn(N, K, generator=g).bfloat16()
+    ref = a.double() @ b.double().T
+    out = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), out, bn=bn)
+    got = out.cpu().double()
+    assert torch.max(torch.abs(got - ref)).item() <= 1e-4 * max(1.0, torch.max(torch.abs(ref)).item()) * (K ** 0.5)
+
+
+def test_gemm_epilogues(gpu):
+    V = gpu
+    import torch
+    g = torch.Generator().manual_seed(5)
+    M, N, K = 384, 64, 192
+    a = torch.randn(M, K, generator=g).bfloat16()
+    b = torch.randn(N, K, generator=g).bfloat16()
+    bias = torch.randn(N, generator=g).float()
+    ref = a.double() @ b.double().T + bias.double()
+    out = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), out, flags=EPI_BIAS | EPI_RELU | EPI_BF16, bias=bias.cuda(), bn=64)
+    expect = torch.clamp(ref, min=0).float().bfloat16().double()
+    assert torch.max(torch.abs(out.cpu().double() - expect)).item() <= 0.02 * torch.max(torch.abs(expect)).item()
+    acc = torch.ones(M, N, dtype=torch.float32, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), acc, flags=EPI_ACCUM, bn=64)
+    ref2 = 1.0 + a.double() @ b.double().T
+    assert torch.max(torch.abs(acc.cpu().double() - ref2)).item() <= 1e-3 * torch.max(torch.abs(ref2)).item()

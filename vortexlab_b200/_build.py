@@ -48,6 +48,7 @@ def _sources(defines=()):
         ("vl_step_f64.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_step_f64.cu")]),
         ("vl_step_lp.o", [nvcc] + cu_flags + inc + ["-c", os.path.join(CSRC, "vl_step_lp.cu")]),
         ("vl_batch.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_batch.cu")]),
+        ("vl_nn.o", [nvcc] + cu_flags + inc + ["-c", os.path.join(CSRC, "vl_nn.cu")]),
         ("vl_noalloc.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_noalloc.cu")]),
     ]
     return jobs

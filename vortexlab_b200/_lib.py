@@ -141,6 +141,7 @@ def _declare(L):
         "vl_batch_download": (i, [vp, i, P(d)]),
         "vl_batch_flags": (i, [vp, i, P(C.c_uint8)]),
         "vl_batch_state_hash": (i, [vp, i, P(u64)]),
+        "vl_nn_gemm_bf16": (i, [vp, i, vp, i, i, i, i, vp, i, P(f), i, i, P(i), vp]),
         "vl_fft": (i, [P(d), P(d), sz]),
         "vl_mean": (d, [P(d), sz]),
         "vl_rms": (d, [P(d), sz]),
