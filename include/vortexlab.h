@@ -255,7 +255,8 @@ double vl_channel_u_ref(const vl_channel* c);
  * No single reference counterpart: the reference runs one Channel at a time
  * (src/cases/tunnel.rs:52-92). A batch advances many channels of uneven sizes, shapes and Reynolds
  * numbers together on one device, each for its own number of steps; every tunnel follows
- * Channel::step exactly (a tunnel in a batch is bit-identical to the same tunnel run alone). */
+ * Channel::step exactly (in FP64 a tunnel in a batch is bit-identical to the same tunnel run alone;
+ * in FP32 / FP16 it agrees to rounding: multiply-add contraction may differ between the kernels). */
 typedef struct vl_batch vl_batch;
 vl_batch* vl_batch_new(int precision);
 void vl_batch_free(vl_batch* b);
@@ -284,6 +285,17 @@ int vl_batch_status(vl_batch* b, int k, uint64_t* t, int* nonfinite, double* for
 int vl_batch_force_history(vl_batch* b, int k, double* out, uint64_t* count);
 /* FP64 populations of tunnel k (reference layout, 9 * nx * ny values), its flags, its state hash. */
 int vl_batch_download(vl_batch* b, int k, double* out);
+/* Ends tunnel k after `steps` steps instead of the count it was added with (which stays the upper
+ * bound and sizes its force history); allowed while the tunnel has not run past `steps`. Lets a
+ * caller stop each tunnel at a moment it picks from the tunnel's own force history. */
+int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps);
+/* Density and velocity of every cell of tunnel k at its current step (solids (1, 0, 0)), FP64,
+ * row-major n = nx * ny values each: Sim::macros (src/sim.rs:527-536) over the whole grid. */
+int vl_batch_macros_field(vl_batch* b, int k, double* rho, double* ux, double* uy);
+/* Sim::init (src/sim.rs:357-371) for tunnel k of a built batch before its first step: the
+ * equilibria of the FP64 fields rho, ux, uy (n = nx * ny values each, row-major) into both
+ * population buffers, solids at rest. The warm-start hook of the batched engine. */
+int vl_batch_init(vl_batch* b, int k, const double* rho, const double* ux, const double* uy);
 int vl_batch_flags(vl_batch* b, int k, uint8_t* out);
 int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
 
@@ -297,6 +309,31 @@ int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
  * timed out waiting for its data. Asynchronous on `stream`. */
 int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N, int K, void* out, int ldc,
                     const float* bias, int flags, int bn, int* err, void* stream);
+/* Gathers and elementwise kernels around the GEMM. Activations are NHWC BF16 (row = pixel,
+ * channels contiguous); a 3x3 convolution (padding 1, stride 1 or 2) is im2col + GEMM, with the
+ * im2col row in (ky, kx, c) order zero-padded to kp (a multiple of 64) columns. */
+int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, void* cols, void* stream);
+int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,
+                 void* stream);
+/* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and transposed [C, R]. */
+int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, void* stream);
+int vl_nn_bias_grad(const void* dzt, int R, int C, float* db, void* stream);
+int vl_nn_transpose_bf16(const void* a, int R, int C, void* at, void* stream);
+/* Nearest 2x upsampling into channels [coff, coff + C) of a ctot-channel output, and its adjoint. */
+int vl_nn_up2(const void* x, int B, int H, int W, int C, void* y, int ctot, int coff, void* stream);
+int vl_nn_up2_bwd(const float* dy, int B, int H, int W, int C, int ctot, int coff, float* dx, int accumulate,
+                  void* stream);
+int vl_nn_copy_channels(const void* x, long long R, int C, void* y, int ctot, int coff, void* stream);
+int vl_nn_slice_channels(const float* y, long long R, int ctot, int coff, int C, float* x, int accumulate, void* stream);
+/* Weighted mean-squared error of out [R, C] against tgt [R, cuse] on the first cuse channels (w
+ * per row): per-block FP64 partial sums of sum(w (out - tgt)^2) * inv_count and the gradient
+ * 2 w (out - tgt) * inv_count (zero on channels cuse..C-1). */
+int vl_nn_mse(const float* out, const float* tgt, const float* w, long long R, int C, int cuse, double inv_count,
+              float* dout, double* partial, int blocks, void* stream);
+/* Adam step `step` (1-based) on FP32 weights; wb (may be NULL) receives a BF16 copy. */
+int vl_nn_adam(float* w, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+               int step, void* wb, void* stream);
+int vl_nn_f32_to_bf16(const float* a, long long n, void* b, void* stream);
 
 /* ================================================================ signal: src/signal.rs */
 int vl_fft(double* re, double* im, size_t n);                              /* :6-44 */

@@ -1,6 +1,7 @@
 """Batched tunnels: a tunnel advanced in a batch with others of other sizes, shapes and Reynolds
-numbers is bit-identical to the same tunnel run alone (state and per-step force), in every tile
-shape and kernel schedule; autotuning does not perturb the run."""
+numbers matches the same tunnel run alone (state and per-step force), in every tile shape and
+kernel schedule (bit-identical in FP64; the FP32 kernels may fuse multiply-adds differently from
+the single-tunnel ones); autotuning does not perturb the run."""
 import numpy as np
 import pytest
 
@@ -24,8 +25,9 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
         ch = c.tunnel.build(c.body)
         ch.sim.record(c.steps)
         ch.step(c.steps)
-        single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy()))
+        single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.populations().copy()))
         ch.close()
+    first = None
     for tile, sched in [("256x1", "concurrent"), ("64x4", "links-first"), ("32x8", "bulk-first")]:
         b = Batch(prec)
         for c in cases:
@@ -34,11 +36,20 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
         b.tile = tile
         b.schedule = sched
         b.run()
+        hashes = []
         for k, c in enumerate(cases):
             t, nonfinite, _ = b.status(k)
             assert t == c.steps and not nonfinite
-            assert b.state_hash(k) == single[k][0], (tile, sched, k)
-            assert np.array_equal(b.force_history(k), single[k][1]), (tile, sched, k)
+            hashes.append(b.state_hash(k))
+            if prec == "f64":
+                assert hashes[-1] == single[k][0], (tile, sched, k)
+                assert np.array_equal(b.force_history(k), single[k][1]), (tile, sched, k)
+            else:
+                assert np.max(np.abs(b.populations(k) - single[k][2])) <= 1e-6, (tile, sched, k)
+                h = b.force_history(k)
+                assert np.max(np.abs(h - single[k][1])) <= 1e-4 * np.max(np.abs(single[k][1])), (tile, sched, k)
+        first = first or hashes
+        assert hashes == first, (tile, sched)      # every tile shape and schedule: bit-identical
         b.close()
 
 
@@ -63,3 +74,78 @@ def test_batch_autotune_and_partial_runs_do_not_change_results(gpu):
         assert b.launch_count() >= 2 * max(c.steps for c in cases)
         b.close()
     assert out[0] == out[1]
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_batch_init_and_macros_match_single_runs(gpu, prec):
+    """A tunnel of the warm form (no ramp, no twist) initialised in a batch from given fields
+    matches the same channel initialised alone with Sim::init: bit-identical in FP64; in FP32 the
+    reduced-precision kernels are compiled with multiply-add contraction, which the compiler may
+    place differently in the batched and the single-tunnel kernel, so the two agree to rounding."""
+    V = gpu
+    from vortexlab_b200 import Channel
+    from vortexlab_b200.batch import Batch
+    cases = _cases(V)
+    fields = []
+    for k, c in enumerate(cases):
+        nx, ny = c.tunnel.grid()
+        X, Y = np.meshgrid(np.arange(nx), np.arange(ny))
+        u = c.tunnel.u
+        fields.append((1.0 + 1e-3 * np.sin(X / 7.0 + k), u * (1.0 + 0.2 * np.cos(Y / 5.0)), 0.1 * u * np.sin(X / 9.0)))
+    single = []
+    for c, f in zip(cases, fields):
+        ch = Channel(c.tunnel.spec_warm(c.body), precision=prec)
+        ch.sim.init(f)
+        ch.sim.record(c.steps)
+        ch.step(c.steps)
+        single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.macros_field()))
+        ch.close()
+    b = Batch(prec)
+    for c in cases:
+        b.add(c.tunnel.spec_warm(c.body), c.steps)
+    b.build()
+    for k, f in enumerate(fields):
+        b.init(k, *f)
+    b.run()
+    with pytest.raises(V.VortexError):
+        b.init(0, *fields[0])
+    for k in range(len(cases)):
+        if prec == "f64":
+            assert b.state_hash(k) == single[k][0], k
+            assert np.array_equal(b.force_history(k), single[k][1]), k
+            for a, s in zip(b.macros_field(k), single[k][2]):
+                assert np.array_equal(a, s), k
+        else:
+            h = b.force_history(k)
+            assert np.max(np.abs(h - single[k][1])) <= 1e-4 * np.max(np.abs(single[k][1])), k
+            for a, s in zip(b.macros_field(k), single[k][2]):
+                assert np.max(np.abs(a - s)) <= 1e-5, k
+    b.close()
+
+
+def test_batch_set_steps_matches_a_shorter_run(gpu):
+    """Ending a running tunnel early (vl_batch_set_steps) gives the state and history of a tunnel
+    added with that many steps; the others are untouched; a tunnel cannot be ended in its past."""
+    V = gpu
+    from vortexlab_b200.batch import Batch
+    cases = _cases(V)
+    ref = Batch("f32")
+    for k, c in enumerate(cases):
+        ref.add(c.tunnel.spec(c.body), 40 if k == 0 else c.steps)
+    ref.build()
+    ref.run()
+    b = Batch("f32")
+    for c in cases:
+        b.add(c.tunnel.spec(c.body), c.steps)
+    b.build()
+    b.run(25)
+    b.set_steps(0, 40)
+    with pytest.raises(V.VortexError):
+        b.set_steps(1, 10)
+    with pytest.raises(V.VortexError):
+        b.set_steps(2, cases[2].steps + 1)
+    b.run()
+    assert b.info(0)["steps"] == 40 and b.status(0)[0] == 40
+    for k in range(len(cases)):
+        assert b.state_hash(k) == ref.state_hash(k), k
+        assert np.array_equal(b.force_history(k), ref.force_history(k)), k

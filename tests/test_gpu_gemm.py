@@ -26,7 +26,9 @@ def _gemm(V, a, b, out, flags=0, bias=None, bn=128):
 
 
 @pytest.mark.parametrize("M,N,K,bn", [(128, 32, 64, 32), (256, 64, 128, 64), (300, 200, 1000, 128),
-                                      (1000, 256, 576, 256), (130, 96, 72, 32), (4096, 128, 288, 128)])
+                                      (1000, 256, 576, 256), (130, 96, 72, 32), (4096, 128, 288, 128),
+                                      (32, 320, 4096, 256), (4096, 320, 16, 256), (512, 8, 64, 32),
+                                      (2048, 64, 8, 64)])
 def test_gemm_matches_fp64(gpu, M, N, K, bn):
     V = gpu
     import torch
@@ -57,3 +59,24 @@ def test_gemm_epilogues(gpu):
     _gemm(V, a.cuda(), b.cuda(), acc, flags=EPI_ACCUM, bn=64)
     ref2 = 1.0 + a.double() @ b.double().T
     assert torch.max(torch.abs(acc.cpu().double() - ref2)).item() <= 1e-3 * torch.max(torch.abs(ref2)).item()
+
+
+def test_gemm_split_k_accumulates(gpu):
+    """Few output tiles over a long K run as split-K partial tiles summed in a fixed order; the
+    accumulate flag adds the sum to the output."""
+    V = gpu
+    import torch
+    g = torch.Generator().manual_seed(8)
+    M, N, K = 40, 96, 8192
+    a = torch.randn(M, K, generator=g).bfloat16()
+    b = torch.randn(N, K, generator=g).bfloat16()
+    ref = a.double() @ b.double().T
+    out = torch.full((M, N), 2.0, dtype=torch.float32, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), out, flags=EPI_ACCUM, bn=128)
+    got = out.cpu().double() - 2.0
+    assert torch.max(torch.abs(got - ref)).item() <= 1e-4 * torch.max(torch.abs(ref)).item() * (K ** 0.5)
+    again = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), again, bn=128)
+    again2 = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    _gemm(V, a.cuda(), b.cuda(), again2, bn=128)
+    assert torch.equal(again, again2)

@@ -139,9 +139,24 @@ def _declare(L):
         "vl_batch_status": (i, [vp, i, P(u64), P(i), P(d)]),
         "vl_batch_force_history": (i, [vp, i, P(d), P(u64)]),
         "vl_batch_download": (i, [vp, i, P(d)]),
+        "vl_batch_init": (i, [vp, i, P(d), P(d), P(d)]),
+        "vl_batch_set_steps": (i, [vp, i, C.c_uint64]),
+        "vl_batch_macros_field": (i, [vp, i, P(d), P(d), P(d)]),
         "vl_batch_flags": (i, [vp, i, P(C.c_uint8)]),
         "vl_batch_state_hash": (i, [vp, i, P(u64)]),
         "vl_nn_gemm_bf16": (i, [vp, i, vp, i, i, i, i, vp, i, P(f), i, i, P(i), vp]),
+        "vl_nn_im2col": (i, [vp, i, i, i, i, i, i, vp, vp]),
+        "vl_nn_col2im": (i, [vp, i, i, i, i, i, i, vp, i, vp]),
+        "vl_nn_act_bwd": (i, [vp, vp, i, i, i, vp, vp, vp]),
+        "vl_nn_bias_grad": (i, [vp, i, i, vp, vp]),
+        "vl_nn_transpose_bf16": (i, [vp, i, i, vp, vp]),
+        "vl_nn_up2": (i, [vp, i, i, i, i, vp, i, i, vp]),
+        "vl_nn_up2_bwd": (i, [vp, i, i, i, i, i, i, vp, i, vp]),
+        "vl_nn_copy_channels": (i, [vp, C.c_longlong, i, vp, i, i, vp]),
+        "vl_nn_slice_channels": (i, [vp, C.c_longlong, i, i, i, vp, i, vp]),
+        "vl_nn_mse": (i, [vp, vp, vp, C.c_longlong, i, i, d, vp, vp, i, vp]),
+        "vl_nn_adam": (i, [vp, vp, vp, vp, C.c_longlong, f, f, f, f, i, vp, vp]),
+        "vl_nn_f32_to_bf16": (i, [vp, C.c_longlong, vp, vp]),
         "vl_fft": (i, [P(d), P(d), sz]),
         "vl_mean": (d, [P(d), sz]),
         "vl_rms": (d, [P(d), sz]),

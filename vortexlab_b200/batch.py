@@ -3,8 +3,10 @@ used to exercise it.
 
 ``Batch`` packs channels of uneven sizes, shapes and Reynolds numbers into one device arena and
 advances them together, each for its own number of steps; every tunnel follows Channel::step
-(src/cases/channel.rs:118-130) exactly, so a tunnel in a batch is bit-identical to the same tunnel
-run alone. ``seeded_tunnels`` draws the bodies and flow parameters of the batched workload.
+(src/cases/channel.rs:118-130) exactly, so in FP64 a tunnel in a batch is bit-identical to the same
+tunnel run alone (in FP32 / FP16 it agrees to rounding: those kernels are compiled with multiply-add
+contraction, which the compiler may place differently in the batched and the single kernels).
+``seeded_tunnels`` draws the bodies and flow parameters of the batched workload.
 """
 from __future__ import annotations
 
@@ -127,6 +129,27 @@ class Batch:
         out = np.zeros(9 * i["nx"] * i["ny"])
         check(lib.vl_batch_download(self._h, k, _dp(out)))
         return out.reshape(9, i["ny"], i["nx"])
+
+    def set_steps(self, k, steps: int):
+        """Ends tunnel k after `steps` steps (at most the count it was added with, not before the
+        current global step)."""
+        check(lib.vl_batch_set_steps(self._h, k, int(steps)))
+
+    def macros_field(self, k):
+        """(rho, ux, uy), each (ny, nx), of tunnel k at its current step."""
+        i = self.info(k)
+        n = i["nx"] * i["ny"]
+        rho, ux, uy = np.zeros(n), np.zeros(n), np.zeros(n)
+        check(lib.vl_batch_macros_field(self._h, k, _dp(rho), _dp(ux), _dp(uy)))
+        return tuple(a.reshape(i["ny"], i["nx"]) for a in (rho, ux, uy))
+
+    def init(self, k, rho, ux, uy):
+        """Sim::init of tunnel k from (ny, nx) fields, before the batch's first step."""
+        i = self.info(k)
+        shape = (i["ny"], i["nx"])
+        arrs = [np.ascontiguousarray(np.broadcast_to(np.asarray(a, np.float64), shape)).reshape(-1)
+                for a in (rho, ux, uy)]
+        check(lib.vl_batch_init(self._h, k, *(_dp(a) for a in arrs)))
 
     def flags(self, k) -> np.ndarray:
         i = self.info(k)

@@ -88,17 +88,23 @@ def plain_runs(cases, tol=0.005):
 
 
 def batched_run(cases, refs, precision="f32", tol=0.005, warm=None, autotune=True):
-    """All cases in one batch. `warm(case) -> (rho, ux, uy)` arrays optionally give start fields.
-    Returns (per-case dicts, total wall seconds, batch info)."""
+    """All cases in one batch. With `warm` (a trained warmstart.UNet) every tunnel runs in its warm
+    form (no ramp, no twist) from the network's prediction; the inference and upload time is
+    counted in the wall time. Returns (per-case dicts, total wall seconds, batch info)."""
     from .batch import Batch
-    b = Batch(precision)
-    for c in cases:
-        b.add(c.tunnel.spec(c.body), c.steps)
-    b.build()
+    t_init = 0.0
+    if warm is not None:
+        from .warmstart import warm_batch
+        b, t_init = warm_batch(warm, cases, precision)
+    else:
+        b = Batch(precision)
+        for c in cases:
+            b.add(c.tunnel.spec(c.body), c.steps)
+        b.build()
     tune = b.autotune(3) if autotune else None
     t0 = time.perf_counter()
     b.run()
-    wall = time.perf_counter() - t0
+    wall = time.perf_counter() - t0 + t_init
     out = []
     total_lu = 0
     for k, c in enumerate(cases):
@@ -116,7 +122,7 @@ def batched_run(cases, refs, precision="f32", tol=0.005, warm=None, autotune=Tru
                         cd_err=(cd_f - r["cd_ref"]) / abs(r["cd_ref"]),
                         st_err=(st_f - r["st_ref"]) / r["st_ref"] if r["st_ref"] else float("nan")))
     binfo = dict(tile=b.tile, autotune_ms_per_step=tune, device_ms=b.last_run_ms(), launches=b.launch_count(),
-                 mlups=total_lu / (b.last_run_ms() * 1e-3) / 1e6)
+                 mlups=total_lu / (b.last_run_ms() * 1e-3) / 1e6, init_s=t_init)
     b.close()
     return out, wall, binfo
 
@@ -154,6 +160,49 @@ def study(subset=32, seed=0x5EED0004, count=256, precision="f32", tol=0.005):
                    max_abs_cd_err=float(max(abs(r["cd_err"]) for r in rows)),
                    max_abs_st_err=float(max(abs(r["st_err"]) for r in rows)),
                    plain_total_s=sum(r["wall_s"] for r in refs), batch_wall_s=wall, batch=binfo)
+    return dict(summary=summary, rows=rows)
+
+
+def warm_comparison(net, cases, refs=None, precision="f32", tol=0.005):
+    """Time to converged c_D and St for the plain form (FP64, one tunnel at a time, uniform start),
+    the batched form from a uniform start and the batched form from the network's warm start.
+    Wall time of a batched tunnel: its steps to convergence x its cells x the batch's seconds per
+    cell update (inference and upload included for the warm form)."""
+    refs = refs if refs is not None else plain_runs(cases, tol=tol)
+    arms = {}
+    for name, w in (("cold", None), ("warm", net)):
+        res, wall, binfo = batched_run(cases, refs, precision=precision, tol=tol, warm=w)
+        total = sum(c.tunnel.grid()[0] * c.tunnel.grid()[1] * c.steps for c in cases)
+        arms[name] = (res, wall / total, binfo)
+    rows = []
+    for k, (c, r) in enumerate(zip(cases, refs)):
+        nx, ny = c.tunnel.grid()
+        row = dict(kind=c.kind, d=c.params["d"], re=round(c.params["re"], 1), steps=c.steps, cd_ref=r["cd_ref"],
+                   st_ref=r["st_ref"], plain_conv_steps=r["conv_steps"],
+                   plain_s=r["wall_s"] / r["steps"] * r["conv_steps"] if r["conv_steps"] >= 0 else None)
+        for name, (res, s_lu, _) in arms.items():
+            f = res[k]
+            row[f"{name}_conv_steps"] = f["conv_steps"]
+            row[f"{name}_cd_err"] = f["cd_err"]
+            row[f"{name}_st_err"] = f["st_err"]
+            row[f"{name}_s"] = s_lu * nx * ny * f["conv_steps"] if f["conv_steps"] >= 0 else None
+        rows.append(row)
+
+    def agg(name):
+        ok = [r for r in rows if r["plain_s"] and r[f"{name}_s"]]
+        if not ok:
+            return dict(converged=0)
+        sp = [r["plain_s"] / r[f"{name}_s"] for r in ok]
+        steps = [r[f"{name}_conv_steps"] / r["plain_conv_steps"] for r in ok]
+        return dict(converged=len(ok), median_speedup=float(np.median(sp)),
+                    aggregate_speedup=sum(r["plain_s"] for r in ok) / sum(r[f"{name}_s"] for r in ok),
+                    median_step_ratio=float(np.median(steps)),
+                    max_abs_cd_err=float(max(abs(r[f"{name}_cd_err"]) for r in ok)),
+                    max_abs_st_err=float(max(abs(r[f"{name}_st_err"]) for r in ok)))
+
+    summary = dict(tunnels=len(rows), plain_converged=sum(1 for r in rows if r["plain_s"]),
+                   cold=agg("cold"), warm=agg("warm"),
+                   batch={n: a[2] for n, a in arms.items()})
     return dict(summary=summary, rows=rows)
 
 

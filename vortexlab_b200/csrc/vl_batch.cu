@@ -422,7 +422,7 @@ int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_
   if (nx) *nx = b->plans[k].dom.nx;
   if (ny) *ny = b->plans[k].dom.ny;
   if (fluid) *fluid = b->plans[k].dom.fluid_nodes;
-  if (steps) *steps = b->steps[k];
+  if (steps) *steps = b->built ? b->tun[k].steps : b->steps[k];
   return VL_OK;
 }
 
@@ -523,6 +523,63 @@ int vl_batch_download(vl_batch* b, int k, double* out) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   cudaFree(tmp);
   if (e != cudaSuccess) return cuda_fail(e, "batch download");
+  return VL_OK;
+}
+
+int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps) {
+  if (!b || !b->built || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  vl::BatchTunnel& T = b->tun[k];
+  if (steps < b->s || b->s > T.steps) return fail(VL_EINVAL, "the tunnel has already run past that step");
+  if (steps > b->steps[k]) return fail(VL_EINVAL, "a tunnel cannot run longer than the steps it was added with");
+  if (steps == T.steps) return VL_OK;
+  T.steps = steps;
+  VB_CUDA(cudaMemcpyAsync(&b->d_tun[k].steps, &T.steps, sizeof T.steps, cudaMemcpyHostToDevice, b->stream));
+  VB_CUDA(cudaStreamSynchronize(b->stream));
+  if (b->gexec) {       // the captured steps may cover the new end: capture again
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return VL_OK;
+}
+
+int vl_batch_macros_field(vl_batch* b, int k, double* rho, double* ux, double* uy) {
+  if (!b || !b->built || !rho || !ux || !uy || k < 0 || (size_t)k >= b->tun.size())
+    return fail(VL_EINVAL, "bad arguments");
+  vl::BatchState st;
+  int rc = pull_state(b, k, &st);
+  if (rc) return rc;
+  const size_t n = b->plans[k].dom.n;
+  const vl::BatchTunnel& T = b->tun[k];
+  double* tmp = nullptr;
+  VB_CUDA(cudaMalloc(&tmp, 3 * n * sizeof(double)));
+  cudaError_t e = b->L->macros((int)n, T.ns, b->d_flag + T.cell_off, 0.0, 0.0, b->tunnel_ptr(b->buf[st.t & 1], k), tmp,
+                               tmp + n, tmp + 2 * n, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(rho, tmp, n * 8, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(ux, tmp + n, n * 8, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(uy, tmp + 2 * n, n * 8, cudaMemcpyDeviceToHost, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return cuda_fail(e, "batch macros");
+  return VL_OK;
+}
+
+int vl_batch_init(vl_batch* b, int k, const double* rho, const double* ux, const double* uy) {
+  if (!b || !b->built || !rho || !ux || !uy || k < 0 || (size_t)k >= b->tun.size())
+    return fail(VL_EINVAL, "bad arguments");
+  if (b->s != 0) return fail(VL_EINVAL, "a tunnel can only be initialised before the batch's first step");
+  const size_t n = b->plans[k].dom.n;
+  const vl::BatchTunnel& T = b->tun[k];
+  double* field = nullptr;
+  VB_CUDA(cudaMalloc(&field, 3 * n * sizeof(double)));
+  cudaError_t e = cudaMemcpyAsync(field, rho, n * 8, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(field + n, ux, n * 8, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(field + 2 * n, uy, n * 8, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess)
+    e = b->L->init((int)n, T.ns, b->d_flag + T.cell_off, field, field + n, field + 2 * n, 1.0, 0.0, 0.0,
+                   b->tunnel_ptr(b->buf[0], k), b->tunnel_ptr(b->buf[1], k), b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  cudaFree(field);
+  if (e != cudaSuccess) return cuda_fail(e, "batch init");
   return VL_OK;
 }
 

@@ -8,8 +8,10 @@
 // cells x ty rows); a link work item is a chunk of up to kBlock boundary nodes of a tunnel. The
 // last chunk of a tunnel to finish a step runs that tunnel's epilogue (force reduction in the same
 // fixed order as a single sim, force record, t + 1). The per-node arithmetic is the single-sim
-// code (pull, link_node, collide), so a tunnel in a batch is bit-identical to the same tunnel run
-// alone.
+// code (pull, link_node, collide), so in FP64 (compiled without multiply-add contraction) a tunnel
+// in a batch is bit-identical to the same tunnel run alone; the FP32 / FP16 kernels are compiled
+// with contraction, which may fuse differently here and in the single-sim kernels (last-bit
+// differences).
 #pragma once
 
 #include "vl_device.cuh"

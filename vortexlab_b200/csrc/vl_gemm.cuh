@@ -11,6 +11,9 @@
 //                      32w..32w+31 = tile rows) and apply the epilogue.
 // Every wait on an mbarrier is bounded: on timeout the CTA records an error code and skips its
 // tile instead of waiting forever.
+//
+// Split K: grid.z > 1 gives CTA z the K-blocks [z * kb_per, (z + 1) * kb_per) and its FP32 tile
+// goes to out + z * split_stride (a workspace that the caller then sums in a fixed order).
 #pragma once
 
 #include <cuda.h>
@@ -40,6 +43,7 @@ struct EpiParams {
   int m_valid, n_valid;  // rows / columns of `out` to write (the padded rest is not stored)
   int flags;
   int* err;          // device error word (0 = fine)
+  long long split_stride;  // elements between the partial results of consecutive K splits
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -103,8 +107,8 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16(int bn) {
 
 template <int BN>
 __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
-                                                      const __grid_constant__ CUtensorMap tmB, int kblocks,
-                                                      EpiParams ep) {
+                                                      const __grid_constant__ CUtensorMap tmB, int kblocks_total,
+                                                      int kb_per, EpiParams ep) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "tile N");
   constexpr int A_BYTES = BM * BK * 2;
   constexpr int B_BYTES = BN * BK * 2;
@@ -119,6 +123,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kb_first = blockIdx.z * kb_per;
+  const int kblocks = min(kblocks_total - kb_first, kb_per);   // >= 1: the host sizes the split
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -148,8 +154,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
       if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) { atomicExch(&failed, 1); break; }
       uint8_t* sa = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_2d(&tmA, &full[s], sa, kb * BK, m0);
-      tma_load_2d(&tmB, &full[s], sa + A_BYTES, kb * BK, n0);
+      tma_load_2d(&tmA, &full[s], sa, (kb_first + kb) * BK, m0);
+      tma_load_2d(&tmB, &full[s], sa + A_BYTES, (kb_first + kb) * BK, n0);
       issued = kb + 1;
     }
     if (failed) {
@@ -217,7 +223,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
           float x = __uint_as_float(v[j]);
           if (ep.flags & EPI_BIAS) x += ep.bias[col];
           if (ep.flags & EPI_RELU) x = fmaxf(x, 0.0f);
-          const size_t o = (size_t)row * ep.ldc + col;
+          const size_t o = (size_t)blockIdx.z * ep.split_stride + (size_t)row * ep.ldc + col;
           if (ep.flags & EPI_BF16) {
             ((__nv_bfloat16*)ep.out)[o] = __float2bfloat16_rn(x);
           } else if (ep.flags & EPI_ACCUM) {

@@ -45,6 +45,14 @@ class Tunnel:
                     nu=self.u * self.d / self.re, collision=self.collision, body=body, ramp_steps=int(5.0 * unit),
                     kick=Kick(cx, cy, 0.4 * self.u / self.d, int(5.0 * unit), int(2.0 * unit)))
 
+    def spec_warm(self, body) -> Spec:
+        """The same channel for a run that starts from a developed field: no inflow ramp and no
+        twist of the body (the start field already carries the wake)."""
+        s = self.spec(body)
+        s.ramp_steps = 0
+        s.kick = None
+        return s
+
     def build(self, body) -> Channel:
         """src/cases/tunnel.rs:52-67."""
         return Channel(self.spec(body), precision=self.precision)
