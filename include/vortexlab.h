@@ -313,12 +313,21 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
  * channels contiguous); a 3x3 convolution (padding 1, stride 1 or 2) is im2col + GEMM, with the
  * im2col row in (ky, kx, c) order zero-padded to kp (a multiple of 64) columns. */
 int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, void* cols, void* stream);
+/* The transposed im2col matrix [kp, rows] (rows = B * Ho * Wo, a multiple of 8), the K-major
+ * operand of the weight-gradient GEMM, gathered directly from x. */
+int vl_nn_im2col_t(const void* x, int B, int H, int W, int C, int stride, int kp, void* colst, void* stream);
 int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,
                  void* stream);
-/* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and transposed [C, R]. */
-int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, void* stream);
-int vl_nn_bias_grad(const void* dzt, int R, int C, float* db, void* stream);
+/* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and transposed [C, R]; colsum (may be NULL)
+ * receives per 32-row tile column sums [C][ceil(R / 32)] that vl_nn_bias_grad reduces to db. */
+int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, float* colsum,
+                  void* stream);
+int vl_nn_bias_grad(const float* colsum, int R, int C, float* db, void* stream);
+/* BF16 transpose [R, C] -> [C, R], R and C even. */
 int vl_nn_transpose_bf16(const void* a, int R, int C, void* at, void* stream);
+/* Weights wf [cin, kpf] of the input-gradient convolution of a stride-1 3x3 layer with weights
+ * w [cout, kp]: wf[c, (ky, kx, co)] = w[co, (2 - ky, 2 - kx, c)], so dX = conv3x3(dZ, wf). */
+int vl_nn_flip_weights(const void* w, int cout, int cin, int kp, int kpf, void* wf, void* stream);
 /* Nearest 2x upsampling into channels [coff, coff + C) of a ctot-channel output, and its adjoint. */
 int vl_nn_up2(const void* x, int B, int H, int W, int C, void* y, int ctot, int coff, void* stream);
 int vl_nn_up2_bwd(const float* dy, int B, int H, int W, int C, int ctot, int coff, float* dx, int accumulate,

@@ -87,22 +87,26 @@ def test_batch_init_and_macros_match_single_runs(gpu, prec):
     from vortexlab_b200.batch import Batch
     cases = _cases(V)
     fields = []
+
+    def nsteps(c):        # FP32: few steps, before rounding differences can grow through the flow
+        return c.steps if prec == "f64" else 20
+
     for k, c in enumerate(cases):
         nx, ny = c.tunnel.grid()
         X, Y = np.meshgrid(np.arange(nx), np.arange(ny))
         u = c.tunnel.u
-        fields.append((1.0 + 1e-3 * np.sin(X / 7.0 + k), u * (1.0 + 0.2 * np.cos(Y / 5.0)), 0.1 * u * np.sin(X / 9.0)))
+        fields.append((1.0 + 1e-4 * np.sin(X / 7.0 + k), u * (1.0 + 0.02 * np.cos(Y / 9.0)), 0.01 * u * np.sin(X / 11.0)))
     single = []
     for c, f in zip(cases, fields):
         ch = Channel(c.tunnel.spec_warm(c.body), precision=prec)
         ch.sim.init(f)
-        ch.sim.record(c.steps)
-        ch.step(c.steps)
+        ch.sim.record(nsteps(c))
+        ch.step(nsteps(c))
         single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.macros_field()))
         ch.close()
     b = Batch(prec)
     for c in cases:
-        b.add(c.tunnel.spec_warm(c.body), c.steps)
+        b.add(c.tunnel.spec_warm(c.body), nsteps(c))
     b.build()
     for k, f in enumerate(fields):
         b.init(k, *f)
@@ -110,6 +114,7 @@ def test_batch_init_and_macros_match_single_runs(gpu, prec):
     with pytest.raises(V.VortexError):
         b.init(0, *fields[0])
     for k in range(len(cases)):
+        assert not b.status(k)[1] and np.all(np.isfinite(single[k][1])), k
         if prec == "f64":
             assert b.state_hash(k) == single[k][0], k
             assert np.array_equal(b.force_history(k), single[k][1]), k

@@ -48,6 +48,43 @@ def test_im2col_col2im(gpu, stride, H, W, Cc):
     assert np.max(np.abs(dx.cpu().numpy() - 2 * dref)) < 2e-5
 
 
+@pytest.mark.parametrize("stride,H,W,Cc", [(1, 8, 12, 4), (2, 8, 12, 8), (1, 6, 8, 3)])
+def test_im2col_t_is_the_transpose(gpu, stride, H, W, Cc):
+    V = gpu
+    import torch
+    from vortexlab_b200 import warmstart as WS
+    rng = np.random.default_rng(stride * 10 + Cc)
+    x = rng.standard_normal((2, H, W, Cc)).astype(np.float32)
+    kp = R.kp_for(Cc, 3)
+    Ho, Wo = (H + stride - 1) // stride, (W + stride - 1) // stride
+    colst = torch.zeros(kp, 2 * Ho * Wo, dtype=torch.bfloat16, device="cuda")
+    _ok(V, V.lib.vl_nn_im2col_t(_p(WS.bf16_upload(x)), 2, H, W, Cc, stride, kp, _p(colst), None))
+    assert np.array_equal(colst.float().cpu().numpy().astype(np.float64), R.im2col(R.bf16(x), stride, kp).T)
+
+
+def test_input_gradient_by_mirrored_weights(gpu):
+    """For a stride-1 3x3 layer, im2col(dZ) times the mirrored weights equals col2im(dZ W)."""
+    V = gpu
+    import torch
+    from vortexlab_b200 import warmstart as WS
+    rng = np.random.default_rng(21)
+    B, H, W, cin, cout = 2, 8, 16, 24, 40
+    kp, kpf = R.kp_for(cin, 3), R.kp_for(cout, 3)
+    w = np.zeros((cout, kp), np.float32)
+    w[:, :9 * cin] = rng.standard_normal((cout, 9 * cin))
+    dz = rng.standard_normal((B * H * W, cout)).astype(np.float32)
+    wb, dzb = WS.bf16_upload(w), WS.bf16_upload(dz)
+    wf = torch.zeros(cin, kpf, dtype=torch.bfloat16, device="cuda")
+    _ok(V, V.lib.vl_nn_flip_weights(_p(wb), cout, cin, kp, kpf, _p(wf), None))
+    cols = torch.zeros(B * H * W, kpf, dtype=torch.bfloat16, device="cuda")
+    _ok(V, V.lib.vl_nn_im2col(_p(dzb), B, H, W, cout, 1, kpf, _p(cols), None))
+    dx = torch.zeros(B * H * W, cin, device="cuda")
+    WS.gemm(cols, kpf, wf, kpf, B * H * W, cin, kpf, dx, cin)
+    torch.cuda.synchronize()
+    ref = R.col2im(R.bf16(dz) @ R.bf16(w), (B, H, W, cin), 1).reshape(-1, cin)
+    assert _rel(dx.cpu().numpy(), ref) < 1e-5
+
+
 def test_elementwise_kernels(gpu):
     V = gpu
     import torch
@@ -80,12 +117,13 @@ def test_elementwise_kernels(gpu):
     dz = torch.zeros(Rn, Cn, dtype=torch.bfloat16, device="cuda")
     dzt = torch.zeros(Cn, Rn, dtype=torch.bfloat16, device="cuda")
     gt = torch.from_numpy(g).cuda()
-    _ok(V, V.lib.vl_nn_act_bwd(_p(gt), _p(act), Rn, Cn, 1, _p(dz), _p(dzt), None))
+    colsum = torch.zeros(Cn, (Rn + 31) // 32, device="cuda")
+    _ok(V, V.lib.vl_nn_act_bwd(_p(gt), _p(act), Rn, Cn, 1, _p(dz), _p(dzt), _p(colsum), None))
     expect = R.bf16(g * (act.float().cpu().numpy() > 0))
     assert np.array_equal(dz.float().cpu().numpy(), expect)
     assert np.array_equal(dzt.float().cpu().numpy(), expect.T)
     db = torch.zeros(Cn, device="cuda")
-    _ok(V, V.lib.vl_nn_bias_grad(_p(dzt), Rn, Cn, _p(db), None))
+    _ok(V, V.lib.vl_nn_bias_grad(_p(colsum), Rn, Cn, _p(db), None))
     assert np.allclose(db.cpu().numpy(), expect.sum(axis=0), atol=1e-4)
     tt = torch.zeros(Rn, Cn, dtype=torch.bfloat16, device="cuda")
     _ok(V, V.lib.vl_nn_transpose_bf16(_p(dzt), Cn, Rn, _p(tt), None))

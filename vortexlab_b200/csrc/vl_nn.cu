@@ -188,30 +188,89 @@ namespace {
 
 __global__ void k_im2col(const bf16* __restrict__ x, int B, int H, int W, int C, int stride, int Ho, int Wo, int kp,
                          bf16* __restrict__ cols) {
-  const long long total = (long long)B * Ho * Wo * kp;
+  // one thread per 8 consecutive columns of a row: a single 16-byte load and store when C % 8 == 0
+  const int G = kp >> 3;
+  const long long total = (long long)B * Ho * Wo * G;
+  const bool vec = (C & 7) == 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i % kp);
-    const long long r = i / kp;
-    bf16 v = __float2bfloat16_rn(0.0f);
-    if (k < 9 * C) {
-      const int c = k % C, t = k / C, kx = t % 3, ky = t / 3;
-      const int ox = (int)(r % Wo), oy = (int)((r / Wo) % Ho), b = (int)(r / ((long long)Wo * Ho));
-      const int iy = stride * oy + ky - 1, ix = stride * ox + kx - 1;
-      if (iy >= 0 && iy < H && ix >= 0 && ix < W) v = x[(((long long)b * H + iy) * W + ix) * C + c];
+    const int g = (int)(i % G);
+    const long long r = i / G;
+    const int ox = (int)(r % Wo);
+    const long long q = r / Wo;
+    const int oy = (int)(q % Ho), b = (int)(q / Ho);
+    const int k0 = g * 8;
+    uint4 out = make_uint4(0u, 0u, 0u, 0u);
+    if (vec) {
+      if (k0 < 9 * C) {
+        const int tap = k0 / C, c = k0 - tap * C;
+        const int iy = stride * oy + tap / 3 - 1, ix = stride * ox + tap % 3 - 1;
+        if (iy >= 0 && iy < H && ix >= 0 && ix < W)
+          out = *reinterpret_cast<const uint4*>(x + (((long long)b * H + iy) * W + ix) * C + c);
+      }
+    } else {
+      __align__(16) bf16 v[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = k0 + j;
+        v[j] = __float2bfloat16_rn(0.0f);
+        if (k < 9 * C) {
+          const int tap = k / C, c = k - tap * C;
+          const int iy = stride * oy + tap / 3 - 1, ix = stride * ox + tap % 3 - 1;
+          if (iy >= 0 && iy < H && ix >= 0 && ix < W) v[j] = x[(((long long)b * H + iy) * W + ix) * C + c];
+        }
+      }
+      out = *reinterpret_cast<const uint4*>(v);
     }
-    cols[i] = v;
+    *reinterpret_cast<uint4*>(cols + r * kp + k0) = out;
+  }
+}
+
+// The transpose of the im2col matrix, colst[k, r] = cols[r, k] ([kp, rows]), gathered straight
+// from x: one thread per 8 consecutive rows of one column (a 16-byte store).
+__global__ void k_im2col_t(const bf16* __restrict__ x, int B, int H, int W, int C, int stride, int Ho, int Wo,
+                           int kp, bf16* __restrict__ colst) {
+  const long long rows = (long long)B * Ho * Wo;
+  const long long RG = rows >> 3;
+  const long long total = RG * kp;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const long long rg = i % RG;
+    const int k = (int)(i / RG);
+    __align__(16) bf16 v[8];
+    if (k >= 9 * C) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) v[j] = __float2bfloat16_rn(0.0f);
+    } else {
+      const int tap = k / C, c = k - tap * C;
+      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const long long r = rg * 8 + j;
+        const int ox = (int)(r % Wo);
+        const long long q = r / Wo;
+        const int oy = (int)(q % Ho), b = (int)(q / Ho);
+        const int iy = stride * oy + dy, ix = stride * ox + dx;
+        v[j] = (iy >= 0 && iy < H && ix >= 0 && ix < W) ? x[(((long long)b * H + iy) * W + ix) * C + c]
+                                                       : __float2bfloat16_rn(0.0f);
+      }
+    }
+    *reinterpret_cast<uint4*>(colst + (long long)k * rows + rg * 8) = *reinterpret_cast<const uint4*>(v);
   }
 }
 
 // dX[b, iy, ix, c] = sum over the (oy, ox, ky, kx) that read it of dcols[(b, oy, ox), (ky, kx, c)].
+// One thread per 4 consecutive channels (float4 loads) when C % 4 == 0, else per channel.
 __global__ void k_col2im(const float* __restrict__ dcols, int B, int H, int W, int C, int stride, int Ho, int Wo,
                          int kp, float* __restrict__ dx, int accumulate) {
-  const long long total = (long long)B * H * W * C;
+  const int V = (C & 3) == 0 ? 4 : 1;
+  const int G = C / V;
+  const long long total = (long long)B * H * W * G;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const int c = (int)(i % C);
-    const long long p = i / C;
-    const int ix = (int)(p % W), iy = (int)((p / W) % H), b = (int)(p / ((long long)W * H));
-    float s = 0.0f;
+    const int c = (int)(i % G) * V;
+    const long long p = i / G;
+    const int ix = (int)(p % W);
+    const long long q = p / W;
+    const int iy = (int)(q % H), b = (int)(q / H);
+    float s[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     for (int ky = 0; ky < 3; ++ky) {
       const int ty = iy + 1 - ky;
       if (ty < 0 || ty % stride) continue;
@@ -222,17 +281,25 @@ __global__ void k_col2im(const float* __restrict__ dcols, int B, int H, int W, i
         if (tx < 0 || tx % stride) continue;
         const int ox = tx / stride;
         if (ox >= Wo) continue;
-        s += dcols[(((long long)b * Ho + oy) * Wo + ox) * kp + (ky * 3 + kx) * C + c];
+        const float* src = dcols + (((long long)b * Ho + oy) * Wo + ox) * kp + (ky * 3 + kx) * C + c;
+        if (V == 4) {
+          const float4 v = *reinterpret_cast<const float4*>(src);
+          s[0] += v.x; s[1] += v.y; s[2] += v.z; s[3] += v.w;
+        } else {
+          s[0] += *src;
+        }
       }
     }
-    dx[i] = accumulate ? dx[i] + s : s;
+    float* o = dx + p * C + c;
+    for (int j = 0; j < V; ++j) o[j] = accumulate ? o[j] + s[j] : s[j];
   }
 }
 
 // dz = dy * (y > 0) (ReLU; y is the layer output) or dz = dy (no activation); BF16 copies of dz
-// row-major [R, C] and transposed [C, R] for the two backward GEMMs; db[c] += sum_r dz[r, c].
+// row-major [R, C] and transposed [C, R] for the two backward GEMMs, and colsum[c, t] = the sum of
+// dz over the 32 rows of row tile t (fixed order), from which the bias gradient is reduced.
 __global__ void k_act_bwd(const float* __restrict__ dy, const bf16* __restrict__ y, int R, int C, int relu,
-                          bf16* __restrict__ dz, bf16* __restrict__ dzt) {
+                          bf16* __restrict__ dz, bf16* __restrict__ dzt, float* __restrict__ colsum, int ntiles) {
   __shared__ float tile[32][33];
   const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
@@ -241,23 +308,30 @@ __global__ void k_act_bwd(const float* __restrict__ dy, const bf16* __restrict__
     if (r < R && c < C) {
       v = dy[(long long)r * C + c];
       if (relu && !(__bfloat162float(y[(long long)r * C + c]) > 0.0f)) v = 0.0f;
-      dz[(long long)r * C + c] = __float2bfloat16_rn(v);
+      const bf16 h = __float2bfloat16_rn(v);
+      dz[(long long)r * C + c] = h;
+      v = __bfloat162float(h);
     }
     tile[j][threadIdx.x] = v;
   }
   __syncthreads();
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int c = c0 + j, r = r0 + threadIdx.x;
-    if (c < C && r < R) dzt[(long long)c * R + r] = __float2bfloat16_rn(tile[threadIdx.x][j]);
+    const float v = tile[threadIdx.x][j];
+    if (c < C && r < R) dzt[(long long)c * R + r] = __float2bfloat16_rn(v);
+    float sum = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if (colsum && threadIdx.x == 0 && c < C) colsum[(long long)c * ntiles + blockIdx.y] = sum;
   }
 }
 
-// db[c] = sum_r dz[r, c] from the BF16 transpose (one block per channel, fixed tree).
-__global__ void k_bias_grad(const bf16* __restrict__ dzt, int R, float* __restrict__ db) {
+// db[c] = sum over the row tiles t of colsum[c, t] (one block per channel, fixed tree).
+__global__ void k_bias_grad(const float* __restrict__ colsum, int ntiles, float* __restrict__ db) {
   __shared__ float red[256];
   const int c = blockIdx.x;
   float s = 0.0f;
-  for (int r = threadIdx.x; r < R; r += blockDim.x) s += __bfloat162float(dzt[(long long)c * R + r]);
+  for (int t = threadIdx.x; t < ntiles; t += blockDim.x) s += colsum[(long long)c * ntiles + t];
   red[threadIdx.x] = s;
   __syncthreads();
   for (int k = blockDim.x / 2; k > 0; k >>= 1) {
@@ -267,18 +341,42 @@ __global__ void k_bias_grad(const bf16* __restrict__ dzt, int R, float* __restri
   if (threadIdx.x == 0) db[c] = red[0];
 }
 
-// BF16 transpose [R, C] -> [C, R].
+// BF16 transpose [R, C] -> [C, R] (R and C even): 64 x 64 tiles moved as pairs of elements.
 __global__ void k_transpose_bf16(const bf16* __restrict__ a, int R, int C, bf16* __restrict__ at) {
-  __shared__ bf16 tile[32][34];
-  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int r = r0 + j, c = c0 + threadIdx.x;
-    tile[j][threadIdx.x] = (r < R && c < C) ? a[(long long)r * C + c] : __float2bfloat16_rn(0.0f);
+  __shared__ bf16 tile[64][66];
+  const int c0 = blockIdx.x * 64, r0 = blockIdx.y * 64;
+  for (int j = threadIdx.y; j < 64; j += blockDim.y) {
+    const int r = r0 + j, c = c0 + 2 * threadIdx.x;
+    __nv_bfloat162 v = __floats2bfloat162_rn(0.0f, 0.0f);
+    if (r < R && c < C) v = *reinterpret_cast<const __nv_bfloat162*>(a + (long long)r * C + c);
+    tile[j][2 * threadIdx.x] = v.x;
+    tile[j][2 * threadIdx.x + 1] = v.y;
   }
   __syncthreads();
-  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-    const int c = c0 + j, r = r0 + threadIdx.x;
-    if (c < C && r < R) at[(long long)c * R + r] = tile[threadIdx.x][j];
+  for (int j = threadIdx.y; j < 64; j += blockDim.y) {
+    const int c = c0 + j, r = r0 + 2 * threadIdx.x;
+    if (c < C && r < R) {
+      __nv_bfloat162 v;
+      v.x = tile[2 * threadIdx.x][j];
+      v.y = tile[2 * threadIdx.x + 1][j];
+      *reinterpret_cast<__nv_bfloat162*>(at + (long long)c * R + r) = v;
+    }
+  }
+}
+
+// Weights of the input-gradient convolution of a stride-1 3x3 layer: wf[c, (ky, kx, co)] =
+// w[co, (2 - ky, 2 - kx, c)] (taps mirrored, input and output channels swapped), zero-padded to
+// kpf columns. With it dX = conv3x3(dZ, wf), an im2col of dZ and one GEMM, with no col2im.
+__global__ void k_flip_weights(const bf16* __restrict__ w, int cout, int cin, int kp, int kpf, bf16* __restrict__ wf) {
+  const long long total = (long long)cin * kpf;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % kpf), c = (int)(i / kpf);
+    bf16 v = __float2bfloat16_rn(0.0f);
+    if (k < 9 * cout) {
+      const int tap = k / cout, co = k - tap * cout;
+      v = w[(long long)co * kp + (8 - tap) * cin + c];
+    }
+    wf[i] = v;
   }
 }
 
@@ -390,39 +488,61 @@ extern "C" {
 
 int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, void* cols, void* stream) {
   if (!x || !cols || (stride != 1 && stride != 2) || kp < 9 * C || kp % 64) return fail(VL_EINVAL, "im2col: bad arguments");
+  if (((uintptr_t)x & 15) || ((uintptr_t)cols & 15)) return fail(VL_EINVAL, "im2col: buffers must be 16-byte aligned");
   const int Ho = (H + stride - 1) / stride, Wo = (W + stride - 1) / stride;
-  k_im2col<<<grid_for((long long)B * Ho * Wo * kp), 256, 0, (cudaStream_t)stream>>>(
+  k_im2col<<<grid_for((long long)B * Ho * Wo * (kp / 8)), 256, 0, (cudaStream_t)stream>>>(
       (const bf16*)x, B, H, W, C, stride, Ho, Wo, kp, (bf16*)cols);
   return launch_check("im2col");
 }
 
+int vl_nn_im2col_t(const void* x, int B, int H, int W, int C, int stride, int kp, void* colst, void* stream) {
+  if (!x || !colst || (stride != 1 && stride != 2) || kp < 9 * C) return fail(VL_EINVAL, "im2col_t: bad arguments");
+  const int Ho = (H + stride - 1) / stride, Wo = (W + stride - 1) / stride;
+  const long long rows = (long long)B * Ho * Wo;
+  if (rows % 8 || ((uintptr_t)colst & 15)) return fail(VL_EINVAL, "im2col_t: rows must be a multiple of 8, output 16-byte aligned");
+  k_im2col_t<<<grid_for(rows / 8 * kp), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, B, H, W, C, stride, Ho, Wo, kp,
+                                                                       (bf16*)colst);
+  return launch_check("im2col_t");
+}
+
 int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,
                  void* stream) {
-  if (!dcols || !dx || (stride != 1 && stride != 2) || kp < 9 * C) return fail(VL_EINVAL, "col2im: bad arguments");
+  if (!dcols || !dx || (stride != 1 && stride != 2) || kp < 9 * C || kp % 4) return fail(VL_EINVAL, "col2im: bad arguments");
+  if (((uintptr_t)dcols & 15) || ((uintptr_t)dx & 15)) return fail(VL_EINVAL, "col2im: buffers must be 16-byte aligned");
   const int Ho = (H + stride - 1) / stride, Wo = (W + stride - 1) / stride;
-  k_col2im<<<grid_for((long long)B * H * W * C), 256, 0, (cudaStream_t)stream>>>(dcols, B, H, W, C, stride, Ho, Wo, kp,
-                                                                                 dx, accumulate);
+  const long long work = (long long)B * H * W * ((C & 3) == 0 ? C / 4 : C);
+  k_col2im<<<grid_for(work), 256, 0, (cudaStream_t)stream>>>(dcols, B, H, W, C, stride, Ho, Wo, kp, dx, accumulate);
   return launch_check("col2im");
 }
 
-int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, void* stream) {
+int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, float* colsum,
+                  void* stream) {
   if (!dy || !dz || !dzt || (relu && !y)) return fail(VL_EINVAL, "act_bwd: bad arguments");
   dim3 grid((C + 31) / 32, (R + 31) / 32), block(32, 8);
-  k_act_bwd<<<grid, block, 0, (cudaStream_t)stream>>>(dy, (const bf16*)y, R, C, relu, (bf16*)dz, (bf16*)dzt);
+  k_act_bwd<<<grid, block, 0, (cudaStream_t)stream>>>(dy, (const bf16*)y, R, C, relu, (bf16*)dz, (bf16*)dzt, colsum,
+                                                      (R + 31) / 32);
   return launch_check("act_bwd");
 }
 
-int vl_nn_bias_grad(const void* dzt, int R, int C, float* db, void* stream) {
-  if (!dzt || !db) return fail(VL_EINVAL, "bias_grad: bad arguments");
-  k_bias_grad<<<C, 256, 0, (cudaStream_t)stream>>>((const bf16*)dzt, R, db);
+int vl_nn_bias_grad(const float* colsum, int R, int C, float* db, void* stream) {
+  if (!colsum || !db) return fail(VL_EINVAL, "bias_grad: bad arguments");
+  k_bias_grad<<<C, 256, 0, (cudaStream_t)stream>>>(colsum, (R + 31) / 32, db);
   return launch_check("bias_grad");
 }
 
 int vl_nn_transpose_bf16(const void* a, int R, int C, void* at, void* stream) {
-  if (!a || !at) return fail(VL_EINVAL, "transpose: bad arguments");
-  dim3 grid((C + 31) / 32, (R + 31) / 32), block(32, 8);
+  if (!a || !at || (R & 1) || (C & 1)) return fail(VL_EINVAL, "transpose: bad arguments (R and C must be even)");
+  if (((uintptr_t)a & 3) || ((uintptr_t)at & 3)) return fail(VL_EINVAL, "transpose: buffers must be 4-byte aligned");
+  dim3 grid((C + 63) / 64, (R + 63) / 64), block(32, 8);
   k_transpose_bf16<<<grid, block, 0, (cudaStream_t)stream>>>((const bf16*)a, R, C, (bf16*)at);
   return launch_check("transpose");
+}
+
+int vl_nn_flip_weights(const void* w, int cout, int cin, int kp, int kpf, void* wf, void* stream) {
+  if (!w || !wf || kp < 9 * cin || kpf < 9 * cout) return fail(VL_EINVAL, "flip_weights: bad arguments");
+  k_flip_weights<<<grid_for((long long)cin * kpf), 256, 0, (cudaStream_t)stream>>>((const bf16*)w, cout, cin, kp, kpf,
+                                                                                  (bf16*)wf);
+  return launch_check("flip_weights");
 }
 
 int vl_nn_up2(const void* x, int B, int H, int W, int C, void* y, int ctot, int coff, void* stream) {

@@ -79,7 +79,10 @@ def gemm(a, lda, b, ldb, M, N, K, out, ldc, flags=0, bias=None, err=None):
 
 class Conv:
     """3x3 (padding 1, stride 1 or 2) or 1x1 convolution + bias (+ ReLU) over NHWC BF16
-    activations. Weights [cout, kp], columns in (ky, kx, c) order, zero-padded to kp."""
+    activations. Weights W[cout, kp], columns in (ky, kx, c) order, zero-padded to kp. The FP32
+    master copy, its gradient and the Adam moments are kept transposed, [kp, cout]: the weight
+    gradient is then the GEMM colsT dzT^T with the long kp side on the tensor-core tile's 128 rows,
+    and Adam writes the BF16 [kp, cout] operand directly."""
 
     def __init__(self, cin, cout, stride=1, relu=True, k=3, seed=0):
         torch = _t()
@@ -89,11 +92,11 @@ class Conv:
         g = torch.Generator().manual_seed(seed)
         w = torch.zeros(cout, self.kp)
         w[:, :fan_in] = torch.randn(cout, fan_in, generator=g) * math.sqrt(2.0 / fan_in) * (1.0 if relu else 0.1)
-        self.w = w.cuda()
+        self.wt = w.t().contiguous().cuda()          # FP32 master, [kp, cout]
         self.b = torch.zeros(cout, device="cuda")
-        self.gw = torch.zeros_like(self.w)
+        self.gwt = torch.zeros_like(self.wt)
         self.gb = torch.zeros_like(self.b)
-        self.mw, self.vw = torch.zeros_like(self.w), torch.zeros_like(self.w)
+        self.mw, self.vw = torch.zeros_like(self.wt), torch.zeros_like(self.wt)
         self.mb, self.vb = torch.zeros_like(self.b), torch.zeros_like(self.b)
         self.wb = torch.zeros(cout, self.kp, dtype=torch.bfloat16, device="cuda")
         self.wbt = torch.zeros(self.kp, cout, dtype=torch.bfloat16, device="cuda")
@@ -103,10 +106,20 @@ class Conv:
     def params(self):
         return self.cout * (9 if self.k == 3 else 1) * self.cin + self.cout
 
+    @property
+    def w(self):
+        """FP32 weights [cout, kp] (a view of the transposed master copy)."""
+        return self.wt.t()
+
+    @property
+    def gw(self):
+        """Weight gradient [cout, kp] (a view)."""
+        return self.gwt.t()
+
     def sync_weights(self):
-        """BF16 copies of the FP32 master weights, [cout, kp] and transposed [kp, cout]."""
-        check(lib.vl_nn_f32_to_bf16(_p(self.w), self.w.numel(), _p(self.wb), None))
-        check(lib.vl_nn_transpose_bf16(_p(self.wb), self.cout, self.kp, _p(self.wbt), None))
+        """BF16 copies of the FP32 master weights, [kp, cout] and transposed [cout, kp]."""
+        check(lib.vl_nn_f32_to_bf16(_p(self.wt), self.wt.numel(), _p(self.wbt), None))
+        check(lib.vl_nn_transpose_bf16(_p(self.wbt), self.kp, self.cout, _p(self.wb), None))
 
     def alloc(self, B, h, w):
         torch = _t()
@@ -116,11 +129,18 @@ class Conv:
         bf = dict(dtype=torch.bfloat16, device="cuda")
         self.cols = torch.zeros(self.rows, self.kp, **bf) if self.k == 3 else None
         self.colst = torch.zeros(self.kp, self.rows, **bf)
-        self.dcols = torch.zeros(self.rows, self.kp, dtype=torch.float32, device="cuda") if self.k == 3 else None
+        self.flip = self.k == 3 and self.stride == 1
+        if self.flip:       # input gradient as a convolution of dz with mirrored weights
+            self.kpf = _kp(9 * self.cout)
+            self.dcols = torch.zeros(self.rows, self.kpf, **bf)
+            self.wf = torch.zeros(self.cin, self.kpf, **bf)
+        elif self.k == 3:   # stride 2: dz W^T, then col2im
+            self.dcols = torch.zeros(self.rows, self.kp, dtype=torch.float32, device="cuda")
         self.y = torch.zeros(self.rows, self.cout, **bf) if self.relu else \
             torch.zeros(self.rows, self.cout, dtype=torch.float32, device="cuda")
         self.dz = torch.zeros(self.rows, self.cout, **bf)
         self.dzt = torch.zeros(self.cout, self.rows, **bf)
+        self.colsum = torch.zeros(self.cout, (self.rows + 31) // 32, dtype=torch.float32, device="cuda")
 
     def forward(self, x, err):
         """x: BF16 [B, h, w, cin] (contiguous). Returns y: BF16 (ReLU layers) or FP32 [rows, cout]."""
@@ -138,14 +158,22 @@ class Conv:
         """dy: FP32 [rows, cout], the gradient of the layer output. Writes (or, with `accumulate`,
         adds) the input gradient into dx (FP32 [B, h, w, cin]); sets gw and gb."""
         check(lib.vl_nn_act_bwd(_p(dy), _p(self.y) if self.relu else None, self.rows, self.cout, int(self.relu),
-                                _p(self.dz), _p(self.dzt), None))
-        check(lib.vl_nn_bias_grad(_p(self.dzt), self.rows, self.cout, _p(self.gb), None))
-        a = self.cols if self.k == 3 else self.x
-        check(lib.vl_nn_transpose_bf16(_p(a), self.rows, self.kp, _p(self.colst), None))
-        gemm(self.dzt, self.rows, self.colst, self.rows, self.cout, self.kp, self.rows, self.gw, self.kp, 0, None, err)
+                                _p(self.dz), _p(self.dzt), _p(self.colsum), None))
+        check(lib.vl_nn_bias_grad(_p(self.colsum), self.rows, self.cout, _p(self.gb), None))
+        if self.k == 3:
+            check(lib.vl_nn_im2col_t(_p(self.x), self.B, self.h, self.wd, self.cin, self.stride, self.kp,
+                                     _p(self.colst), None))
+        else:
+            check(lib.vl_nn_transpose_bf16(_p(self.x), self.rows, self.kp, _p(self.colst), None))
+        gemm(self.colst, self.rows, self.dzt, self.rows, self.kp, self.cout, self.rows, self.gwt, self.cout, 0, None, err)
         if not need_dx:
             return
-        if self.k == 3:
+        if self.flip:
+            check(lib.vl_nn_flip_weights(_p(self.wb), self.cout, self.cin, self.kp, self.kpf, _p(self.wf), None))
+            check(lib.vl_nn_im2col(_p(self.dz), self.B, self.ho, self.wo, self.cout, 1, self.kpf, _p(self.dcols), None))
+            gemm(self.dcols, self.kpf, self.wf, self.kpf, self.rows, self.cin, self.kpf, dx, self.cin,
+                 EPI_ACCUM if accumulate else 0, None, err)
+        elif self.k == 3:
             gemm(self.dz, self.cout, self.wbt, self.cout, self.rows, self.kp, self.cout, self.dcols, self.kp, 0, None,
                  err)
             check(lib.vl_nn_col2im(_p(self.dcols), self.B, self.h, self.wd, self.cin, self.stride, self.kp, _p(dx),
@@ -155,11 +183,11 @@ class Conv:
                  EPI_ACCUM if accumulate else 0, None, err)
 
     def adam(self, step, lr, b1=0.9, b2=0.999, eps=1e-8):
-        check(lib.vl_nn_adam(_p(self.w), _p(self.gw), _p(self.mw), _p(self.vw), self.w.numel(), lr, b1, b2, eps,
-                             step, _p(self.wb), None))
+        check(lib.vl_nn_adam(_p(self.wt), _p(self.gwt), _p(self.mw), _p(self.vw), self.wt.numel(), lr, b1, b2, eps,
+                             step, _p(self.wbt), None))
         check(lib.vl_nn_adam(_p(self.b), _p(self.gb), _p(self.mb), _p(self.vb), self.b.numel(), lr, b1, b2, eps,
                              step, None, None))
-        check(lib.vl_nn_transpose_bf16(_p(self.wb), self.cout, self.kp, _p(self.wbt), None))
+        check(lib.vl_nn_transpose_bf16(_p(self.wbt), self.kp, self.cout, _p(self.wb), None))
 
 
 class UNet:
@@ -289,7 +317,7 @@ class UNet:
     def load(self, st):
         torch = _t()
         for i, c in enumerate(self.layers()):
-            c.w.copy_(torch.from_numpy(np.asarray(st[f"w{i}"], np.float32)))
+            c.wt.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(st[f"w{i}"], np.float32).T)))
             c.b.copy_(torch.from_numpy(np.asarray(st[f"b{i}"], np.float32)))
             c.sync_weights()
 
