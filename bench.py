@@ -184,6 +184,31 @@ def channel_n80(V):
     return out
 
 
+def time_to_converged():
+    """The second half of the headline metric on a bounded sample: time to converged c_D and St of
+    the fast form (FP32, batched, learned warm start with the shipped network) and of the batched
+    form from a uniform start, each against the plain FP64 GPU path (one tunnel at a time), on 8
+    held-out tunnels (D <= 22, Re >= 100) for 100 convective units."""
+    from vortexlab_b200 import convergence as CV
+    from vortexlab_b200 import warmstart as WS
+    from vortexlab_b200.batch import seeded_tunnels
+    cases = [c for c in seeded_tunnels(seed=WS.TEST_SEED, count=256, units=100.0)
+             if c.params["d"] <= 22 and c.params["re"] >= 100.0][:8]
+    t0 = time.perf_counter()
+    out = CV.warm_comparison(WS.load_pretrained(), cases)
+    s = out["summary"]
+
+    def arm(a):
+        return {k: (float(f"{a[k]:.4g}") if isinstance(a.get(k), float) else a.get(k))
+                for k in ("converged", "median_speedup", "aggregate_speedup", "median_step_ratio",
+                          "max_abs_cd_err", "max_abs_st_err")}
+    return {"sample": "8 held-out tunnels of seed 0x5EED0004 with D <= 22 and Re >= 100, 100 convective units",
+            "criterion": "every later 3-period window within 0.5 % of the plain FP64 run on mean c_D and St",
+            "plain_converged": s["plain_converged"], "fast_form": arm(s["warm"]), "uniform_start_batched": arm(s["cold"]),
+            "seconds": round(time.perf_counter() - t0, 1),
+            "full_study": "200 held-out tunnels: 7.8x median, 5.6x aggregate (profiles/warmstart_study.md)"}
+
+
 def run_vortexlab(args):
     import numpy as np
 
@@ -287,6 +312,7 @@ def run_vortexlab(args):
     sim.close()
     if rank == 0 and world == 1 and not args.no_extras:
         line["channel_n80"] = channel_n80(V)
+        line["time_to_converged"] = time_to_converged()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         mlups, steps, secs = time_oracle(threads, 50, budget_s=15.0)

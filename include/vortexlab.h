@@ -313,9 +313,6 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
  * channels contiguous); a 3x3 convolution (padding 1, stride 1 or 2) is im2col + GEMM, with the
  * im2col row in (ky, kx, c) order zero-padded to kp (a multiple of 64) columns. */
 int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, void* cols, void* stream);
-/* The transposed im2col matrix [kp, rows] (rows = B * Ho * Wo, a multiple of 8), the K-major
- * operand of the weight-gradient GEMM, gathered directly from x. */
-int vl_nn_im2col_t(const void* x, int B, int H, int W, int C, int stride, int kp, void* colst, void* stream);
 int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,
                  void* stream);
 /* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and transposed [C, R]; colsum (may be NULL)

@@ -48,20 +48,6 @@ def test_im2col_col2im(gpu, stride, H, W, Cc):
     assert np.max(np.abs(dx.cpu().numpy() - 2 * dref)) < 2e-5
 
 
-@pytest.mark.parametrize("stride,H,W,Cc", [(1, 8, 12, 4), (2, 8, 12, 8), (1, 6, 8, 3)])
-def test_im2col_t_is_the_transpose(gpu, stride, H, W, Cc):
-    V = gpu
-    import torch
-    from vortexlab_b200 import warmstart as WS
-    rng = np.random.default_rng(stride * 10 + Cc)
-    x = rng.standard_normal((2, H, W, Cc)).astype(np.float32)
-    kp = R.kp_for(Cc, 3)
-    Ho, Wo = (H + stride - 1) // stride, (W + stride - 1) // stride
-    colst = torch.zeros(kp, 2 * Ho * Wo, dtype=torch.bfloat16, device="cuda")
-    _ok(V, V.lib.vl_nn_im2col_t(_p(WS.bf16_upload(x)), 2, H, W, Cc, stride, kp, _p(colst), None))
-    assert np.array_equal(colst.float().cpu().numpy().astype(np.float64), R.im2col(R.bf16(x), stride, kp).T)
-
-
 def test_input_gradient_by_mirrored_weights(gpu):
     """For a stride-1 3x3 layer, im2col(dZ) times the mirrored weights equals col2im(dZ W)."""
     V = gpu

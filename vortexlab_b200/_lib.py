@@ -146,7 +146,6 @@ def _declare(L):
         "vl_batch_state_hash": (i, [vp, i, P(u64)]),
         "vl_nn_gemm_bf16": (i, [vp, i, vp, i, i, i, i, vp, i, P(f), i, i, P(i), vp]),
         "vl_nn_im2col": (i, [vp, i, i, i, i, i, i, vp, vp]),
-        "vl_nn_im2col_t": (i, [vp, i, i, i, i, i, i, vp, vp]),
         "vl_nn_flip_weights": (i, [vp, i, i, i, i, vp, vp]),
         "vl_nn_col2im": (i, [vp, i, i, i, i, i, i, vp, i, vp]),
         "vl_nn_act_bwd": (i, [vp, vp, i, i, i, vp, vp, vp, vp]),

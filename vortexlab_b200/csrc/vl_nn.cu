@@ -225,38 +225,6 @@ __global__ void k_im2col(const bf16* __restrict__ x, int B, int H, int W, int C,
   }
 }
 
-// The transpose of the im2col matrix, colst[k, r] = cols[r, k] ([kp, rows]), gathered straight
-// from x: one thread per 8 consecutive rows of one column (a 16-byte store).
-__global__ void k_im2col_t(const bf16* __restrict__ x, int B, int H, int W, int C, int stride, int Ho, int Wo,
-                           int kp, bf16* __restrict__ colst) {
-  const long long rows = (long long)B * Ho * Wo;
-  const long long RG = rows >> 3;
-  const long long total = RG * kp;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-    const long long rg = i % RG;
-    const int k = (int)(i / RG);
-    __align__(16) bf16 v[8];
-    if (k >= 9 * C) {
-#pragma unroll
-      for (int j = 0; j < 8; ++j) v[j] = __float2bfloat16_rn(0.0f);
-    } else {
-      const int tap = k / C, c = k - tap * C;
-      const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const long long r = rg * 8 + j;
-        const int ox = (int)(r % Wo);
-        const long long q = r / Wo;
-        const int oy = (int)(q % Ho), b = (int)(q / Ho);
-        const int iy = stride * oy + dy, ix = stride * ox + dx;
-        v[j] = (iy >= 0 && iy < H && ix >= 0 && ix < W) ? x[(((long long)b * H + iy) * W + ix) * C + c]
-                                                       : __float2bfloat16_rn(0.0f);
-      }
-    }
-    *reinterpret_cast<uint4*>(colst + (long long)k * rows + rg * 8) = *reinterpret_cast<const uint4*>(v);
-  }
-}
-
 // dX[b, iy, ix, c] = sum over the (oy, ox, ky, kx) that read it of dcols[(b, oy, ox), (ky, kx, c)].
 // One thread per 4 consecutive channels (float4 loads) when C % 4 == 0, else per channel.
 __global__ void k_col2im(const float* __restrict__ dcols, int B, int H, int W, int C, int stride, int Ho, int Wo,
@@ -493,16 +461,6 @@ int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, 
   k_im2col<<<grid_for((long long)B * Ho * Wo * (kp / 8)), 256, 0, (cudaStream_t)stream>>>(
       (const bf16*)x, B, H, W, C, stride, Ho, Wo, kp, (bf16*)cols);
   return launch_check("im2col");
-}
-
-int vl_nn_im2col_t(const void* x, int B, int H, int W, int C, int stride, int kp, void* colst, void* stream) {
-  if (!x || !colst || (stride != 1 && stride != 2) || kp < 9 * C) return fail(VL_EINVAL, "im2col_t: bad arguments");
-  const int Ho = (H + stride - 1) / stride, Wo = (W + stride - 1) / stride;
-  const long long rows = (long long)B * Ho * Wo;
-  if (rows % 8 || ((uintptr_t)colst & 15)) return fail(VL_EINVAL, "im2col_t: rows must be a multiple of 8, output 16-byte aligned");
-  k_im2col_t<<<grid_for(rows / 8 * kp), 256, 0, (cudaStream_t)stream>>>((const bf16*)x, B, H, W, C, stride, Ho, Wo, kp,
-                                                                       (bf16*)colst);
-  return launch_check("im2col_t");
 }
 
 int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,

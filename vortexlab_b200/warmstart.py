@@ -21,6 +21,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 import time
 from dataclasses import dataclass, field
 
@@ -160,11 +161,8 @@ class Conv:
         check(lib.vl_nn_act_bwd(_p(dy), _p(self.y) if self.relu else None, self.rows, self.cout, int(self.relu),
                                 _p(self.dz), _p(self.dzt), _p(self.colsum), None))
         check(lib.vl_nn_bias_grad(_p(self.colsum), self.rows, self.cout, _p(self.gb), None))
-        if self.k == 3:
-            check(lib.vl_nn_im2col_t(_p(self.x), self.B, self.h, self.wd, self.cin, self.stride, self.kp,
-                                     _p(self.colst), None))
-        else:
-            check(lib.vl_nn_transpose_bf16(_p(self.x), self.rows, self.kp, _p(self.colst), None))
+        a = self.cols if self.k == 3 else self.x
+        check(lib.vl_nn_transpose_bf16(_p(a), self.rows, self.kp, _p(self.colst), None))
         gemm(self.colst, self.rows, self.dzt, self.rows, self.kp, self.cout, self.rows, self.gwt, self.cout, 0, None, err)
         if not need_dx:
             return
@@ -320,6 +318,39 @@ class UNet:
             c.wt.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(st[f"w{i}"], np.float32).T)))
             c.b.copy_(torch.from_numpy(np.asarray(st[f"b{i}"], np.float32)))
             c.sync_weights()
+
+
+PRETRAINED = os.path.join(os.path.dirname(__file__), "data", "warmstart_unet.npz")
+
+
+def save_bf16(net, path):
+    """Writes the network with its weights rounded to BF16 (the values its GEMMs use) and its FP32
+    biases: inference from the file is identical to inference from the network."""
+    out = {}
+    for k, v in net.state().items():
+        if k.startswith("w"):
+            u = np.ascontiguousarray(v, np.float32).view(np.uint32).astype(np.uint64)
+            out[k] = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+        else:
+            out[k] = np.asarray(v, np.float32)
+    out["config"] = np.array([net.levels, net.c0, net.cin, net.cout], np.int32)
+    np.savez_compressed(path, **out)
+
+
+def load_pretrained(path=PRETRAINED):
+    """The network trained on solver-generated wakes (2000 tunnels of seed 0x7EA10001 at 50
+    convective units, stopped on a lift peak): weights stored as BF16, biases FP32."""
+    z = np.load(path)
+    levels, c0, cin, cout = (int(v) for v in z["config"])
+    net = UNet(levels=levels, c0=c0, cin=cin, cout=cout)
+    st = {}
+    for k in z.files:
+        if k.startswith("w"):
+            st[k] = (z[k].astype(np.uint32) << 16).view(np.float32)
+        elif k.startswith("b"):
+            st[k] = z[k]
+    net.load(st)
+    return net
 
 
 # ---------------------------------------------------------------------------- data encodings
@@ -629,7 +660,7 @@ def study(n_train=2000, n_test=200, gen_units=50.0, eval_units=100.0, train_seco
     log(f"trained {tl.steps} steps in {tl.seconds:.1f} s; validation MSE {out['train']['val_mse']:.5f} "
         f"(uniform start {out['train']['val_mse_uniform']:.5f})")
     if weights_out:
-        np.savez(weights_out, **net.state())
+        save_bf16(net, weights_out)
     test = seeded_tunnels(seed=TEST_SEED, count=n_test, units=eval_units)
     t0 = time.perf_counter()
     cmp = CV.warm_comparison(net, test)
@@ -651,6 +682,6 @@ if __name__ == "__main__":
     def log(m):
         print(m, flush=True)
 
-    res = study(**kw, log=log, weights_out=os.path.join(outdir, "warmstart_weights.npz"))
+    res = study(**kw, log=log, weights_out=os.path.join(outdir, "warmstart_unet.npz"))
     with open(os.path.join(outdir, "warmstart_study.json"), "w") as f:
         json.dump(res, f, default=float, indent=1)
