@@ -195,15 +195,22 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
         smem_u32(&done)));
   }
 
-  // Epilogue: every warp waits for the accumulator, then reads its 32 rows.
+  // Epilogue: every warp waits for the accumulator, then reads its 32 rows 32 columns at a time
+  // (lane = row). Each 32 x 32 block goes through shared memory (the idle stage buffers) so that
+  // the global stores are row-contiguous across the warp: lane = column.
   const bool have = mbar_wait(&done, 0);
   asm volatile("tcgen05.fence::after_thread_sync;");
   __syncwarp();
-  const int row = m0 + warp * 32 + lane;
   const bool good = have && !failed;
   if (good) {
+    // the stage buffers were last read by the tensor cores (async proxy): order those reads before
+    // this warp's generic writes to the same memory
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    float* stg = reinterpret_cast<float*>(smem) + warp * (32 * 33);
+    const int rbase = m0 + warp * 32;
 #pragma unroll 1
     for (int c0 = 0; c0 < BN; c0 += 32) {
+      if (n0 + c0 >= ep.n_valid) break;   // same for every warp of the CTA
       uint32_t v[32];
       const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
       asm volatile(
@@ -215,14 +222,19 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
             "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
           : "r"(taddr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (row < ep.m_valid) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int col = n0 + c0 + j;
-          if (col >= ep.n_valid) break;
-          float x = __uint_as_float(v[j]);
-          if (ep.flags & EPI_BIAS) x += ep.bias[col];
-          if (ep.flags & EPI_RELU) x = fmaxf(x, 0.0f);
+      for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = __uint_as_float(v[j]);
+      __syncwarp();
+      const int col = n0 + c0 + lane;
+      const bool cok = col < ep.n_valid;
+      const float bv = (cok && (ep.flags & EPI_BIAS)) ? ep.bias[col] : 0.0f;
+#pragma unroll 4
+      for (int r = 0; r < 32; ++r) {
+        const int row = rbase + r;
+        if (row >= ep.m_valid) break;     // same for every lane
+        float x = stg[r * 33 + lane] + bv;
+        if (ep.flags & EPI_RELU) x = fmaxf(x, 0.0f);
+        if (cok) {
           const size_t o = (size_t)blockIdx.z * ep.split_stride + (size_t)row * ep.ldc + col;
           if (ep.flags & EPI_BF16) {
             ((__nv_bfloat16*)ep.out)[o] = __float2bfloat16_rn(x);
@@ -233,6 +245,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
           }
         }
       }
+      __syncwarp();
     }
   } else if (threadIdx.x == 0 && ep.err) {
     atomicExch(ep.err, 1);
