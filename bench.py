@@ -316,8 +316,11 @@ def run_vortexlab(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         mlups, steps, secs = time_oracle(threads, 50, budget_s=15.0)
+        m1, s1, t1 = time_oracle(1, 20, budget_s=8.0)
         line["cpu_baseline"] = {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
-                                "sample": f"{steps} full steps of the same box after 1 untimed step ({secs:.1f} s)"}
+                                "sample": f"{steps} full steps of the same box after 1 untimed step ({secs:.1f} s)",
+                                "single_thread": {"value": round(m1, 2), "cores": 1,
+                                                  "sample": f"{s1} full steps after 1 untimed step ({t1:.1f} s)"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:

@@ -179,3 +179,19 @@ def test_schedules_and_autotune_do_not_change_results(gpu):
         r.ch.step(150)
         results.append((sim.state_hash(), sim.history().tobytes()))
     assert all(x == results[0] for x in results)
+
+
+@pytest.mark.parametrize("n,published", [
+    (20, (3.3244, 3.2719, 0.9807, -1.0175, 0.2988, 2.4700)),
+    (40, (3.2423, 3.1919, 0.9830, -1.0181, 0.3006, 2.4734)),
+    (80, (3.2354, 3.1840, 0.9947, -1.0295, 0.3007, 2.4840)),
+])
+def test_published_2d2_results(gpu, n, published):
+    """README.md:182-188: the reference's own case-2D-2 results (lattice U 0.05, 100 convective
+    units, statistics over the last 20) at 20, 40 and 80 cells per diameter, to the four decimals
+    it prints: c_D max / min, c_L max / min, St and the pressure drop."""
+    V = gpu
+    u = V.cylinder.run_2d2(V.cylinder.Setup(n=n), 100.0, 20.0)
+    got = (u.cd_max, u.cd_min, u.cl_max, u.cl_min, u.st, u.dp)
+    for name, g, p in zip(("cd_max", "cd_min", "cl_max", "cl_min", "st", "dp"), got, published):
+        assert abs(g - p) <= 1e-4, (name, g, p)

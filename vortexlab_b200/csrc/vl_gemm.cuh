@@ -25,7 +25,7 @@ namespace gemm {
 
 constexpr int BM = 128;      // tile rows (UMMA M)
 constexpr int BK = 64;       // K elements per stage: 128 bytes of BF16 = one swizzle row
-constexpr int STAGES = 4;
+constexpr int STAGES = 4;   // most stages of the shared-memory ring (a launch may use fewer)
 constexpr unsigned kSpinLimit = 1u << 26;  // polls of an mbarrier before giving up
 
 // Epilogue flags.
@@ -108,7 +108,7 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16(int bn) {
 template <int BN>
 __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
                                                       const __grid_constant__ CUtensorMap tmB, int kblocks_total,
-                                                      int kb_per, EpiParams ep) {
+                                                      int kb_per, int stages, EpiParams ep) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "tile N");
   constexpr int A_BYTES = BM * BK * 2;
   constexpr int B_BYTES = BN * BK * 2;
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
   const int kblocks = min(kblocks_total - kb_first, kb_per);   // >= 1: the host sizes the split
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < STAGES; ++s) {
+    for (int s = 0; s < stages; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -149,8 +149,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     // TMA producer.
     int issued = 0;
     for (int kb = 0; kb < kblocks; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t round = (uint32_t)(kb / STAGES);
+      const int s = kb % stages;
+      const uint32_t round = (uint32_t)(kb / stages);
       if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) { atomicExch(&failed, 1); break; }
       uint8_t* sa = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
@@ -160,16 +160,16 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     }
     if (failed) {
       // Drain: wait (bounded) for the copies still in flight before the block can exit.
-      for (int kb = issued > STAGES ? issued - STAGES : 0; kb < issued; ++kb)
-        mbar_wait(&full[kb % STAGES], (uint32_t)(kb / STAGES) & 1u);
+      for (int kb = issued > stages ? issued - stages : 0; kb < issued; ++kb)
+        mbar_wait(&full[kb % stages], (uint32_t)(kb / stages) & 1u);
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer.
     constexpr uint32_t idesc = instr_desc_bf16(BN);
     bool ok = true;
     for (int kb = 0; kb < kblocks && ok; ++kb) {
-      const int s = kb % STAGES;
-      const uint32_t round = (uint32_t)(kb / STAGES);
+      const int s = kb % stages;
+      const uint32_t round = (uint32_t)(kb / stages);
       if (!mbar_wait(&full[s], round & 1u)) { atomicExch(&failed, 1); ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
@@ -256,8 +256,8 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
 }
 
 template <int BN>
-constexpr int smem_bytes() {
-  return STAGES * (BM * BK * 2 + BN * BK * 2) + 1024;
+constexpr int smem_bytes(int stages = STAGES) {
+  return stages * (BM * BK * 2 + BN * BK * 2) + 1024;
 }
 
 }  // namespace gemm

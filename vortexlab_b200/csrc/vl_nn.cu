@@ -132,8 +132,12 @@ int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int 
   } else {
     p.split_stride = 0;
   }
+  // A short K per CTA (the im2col GEMMs of the narrow layers: 1-8 K-blocks) gains nothing from a
+  // deep ring; two stages let 2 (BN 256) to 5 (BN 32) CTAs share an SM instead, so one CTA's
+  // epilogue overlaps the next one's loads. TMEM stays within its 512 columns in both cases.
+  const int stages = kb_per <= 8 ? 2 : vl::gemm::STAGES;
   dim3 grid(gx, gy, splits);
-  vl::gemm::k_gemm_bf16<BN><<<grid, 128, smem, s>>>(ta, tb, kblocks, kb_per, p);
+  vl::gemm::k_gemm_bf16<BN><<<grid, 128, vl::gemm::smem_bytes<BN>(stages), s>>>(ta, tb, kblocks, kb_per, stages, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(VL_ECUDA, std::string("gemm launch: ") + cudaGetErrorString(e));
   if (splits > 1) {
