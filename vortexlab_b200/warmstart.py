@@ -670,14 +670,14 @@ def study(n_train=2000, n_test=200, gen_units=50.0, eval_units=100.0, train_seco
 
 
 if __name__ == "__main__":
-    # python -m vortexlab_b200.warmstart OUTDIR [n_train n_test gen_units eval_units train_seconds]
+    # python -m vortexlab_b200.warmstart OUTDIR [n_train n_test gen_units eval_units train_seconds epochs]
     import json
     import os
     import sys
     outdir = sys.argv[1]
     os.makedirs(outdir, exist_ok=True)
-    names = ["n_train", "n_test", "gen_units", "eval_units", "train_seconds"]
-    kw = {k: (int(v) if k.startswith("n_") else float(v)) for k, v in zip(names, sys.argv[2:])}
+    names = ["n_train", "n_test", "gen_units", "eval_units", "train_seconds", "epochs"]
+    kw = {k: (int(v) if k.startswith("n_") or k == "epochs" else float(v)) for k, v in zip(names, sys.argv[2:])}
 
     def log(m):
         print(m, flush=True)
