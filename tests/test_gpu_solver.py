@@ -1,4 +1,5 @@
-"""The reference's solver-level tests (tests/solver.rs) run on the device, with the reference's
+"""The reference's solver-level tests (tests/solver.rs) and the validation cases of
+tests/validation.rs that need no external data run on the device, with the reference's
 tolerances. Together with the oracle parity tests they show the kernels keep the invariants the
 reference guarantees: conservation, Galilean-invariant wall forces, transparent open boundaries,
 determinism and a working absorbing outlet."""
@@ -176,3 +177,73 @@ def test_under_resolved_2d2_reports_divergence(gpu):
     V = gpu
     with pytest.raises(V.VortexError, match="diverged"):
         V.cylinder.run_2d2(V.cylinder.Setup(n=10), 30.0, 5.0)
+
+
+def _poiseuille(rows, q, collision, tau=0.8):
+    """src/cases/poiseuille.rs:41-90 on the device: the body-force channel run until the profile
+    changes by less than 1e-13 u_max over 200 steps; relative L2 error against the parabola and
+    wall drag over driving force."""
+    d = S.poiseuille(rows=rows, tau=tau, q=q, collision=collision)
+    sim = S.product_sim(d)
+    y0, y1 = 1.0 - q, rows + q
+    nu = (tau - 0.5) / 3.0
+    umax = 0.1 * 16.0 / rows
+    g = d["accel"][0]
+    prev = np.zeros(rows + 2)
+    while True:
+        sim.step(200)
+        u = sim.macros_field()[1][:, 1]
+        change = np.max(np.abs(u[1:rows + 1] - prev[1:rows + 1]))
+        prev = u
+        if change < 1e-13 * umax or sim.t > 4_000_000:
+            break
+    y = np.arange(1, rows + 1, dtype=float)
+    exact = g / (2.0 * nu) * (y - y0) * (y1 - y)
+    num = float(np.sum((u[1:rows + 1] - exact) ** 2))
+    den = float(np.sum(exact ** 2))
+    return dict(rows=rows, q=q, l2=(num / den) ** 0.5, force_balance=sim.force[0][0] / (g * sim.total_mass()))
+
+
+def test_poiseuille_is_second_order_and_exact_with_the_magic_parameter(gpu):
+    """tests/validation.rs:19-36: second-order convergence of the driven channel for BGK and TRT
+    with halfway and off-lattice walls; TRT with Lambda = 3/16 and halfway walls exact to rounding,
+    with the wall drag balancing the driving force."""
+    for collision, q in (("bgk", 0.5), (("trt", 0.25), 0.5), (("trt", 3.0 / 16.0), 0.25), (("trt", 3.0 / 16.0), 0.8)):
+        out = [_poiseuille(h, q, collision) for h in (8, 16, 32)]
+        for a, b in zip(out, out[1:]):
+            h0, h1 = a["rows"] - 1.0 + 2.0 * a["q"], b["rows"] - 1.0 + 2.0 * b["q"]
+            order = np.log(a["l2"] / b["l2"]) / np.log(h1 / h0)
+            assert abs(order - 2.0) < 0.05, (collision, q, order)
+        assert out[2]["l2"] < 2.5e-3, (collision, q, out[2]["l2"])
+    for o in (_poiseuille(h, 0.5, ("trt", 3.0 / 16.0)) for h in (8, 16, 32)):
+        assert o["l2"] < 1e-10, o
+        assert abs(o["force_balance"] - 1.0) < 1e-9, o
+
+
+def test_rounding_the_corners_lowers_drag_and_raises_the_shedding_frequency(gpu):
+    """tests/validation.rs:96-124: a square of side 20 and the same square with corners rounded
+    by 20 % in a towing tank at Re 100 (u 0.1, 10 % blockage), 70 convective units in 20 parts,
+    statistics after 40."""
+    V = gpu
+    from vortexlab_b200.tunnel import Tunnel
+    tn = Tunnel(d=20, re=100.0, u=0.1, upstream=6.0, downstream=12.0, height=10.0)
+    cx, cy = tn.centre()
+
+    def run(corner):
+        ch = tn.build(V.section(corner, cx, cy, 20.0, 0.0))
+        cd, cl = [], []
+        for _ in range(20):
+            s = tn.run(ch, 70.0 / 20.0)
+            cd.append(s.cd)
+            cl.append(s.cl)
+        ch.close()
+        return V.Series(s.dt, np.concatenate(cd), np.concatenate(cl)).stats(40.0)
+
+    square, rounded = run(V.Corner.Sharp), run(V.Corner.Rounded(0.2))
+    assert 1.45 < square.cd_mean < 1.75, square
+    assert 0.14 < square.st < 0.17, square
+    assert 0.1 < square.cl_rms < 0.35, square
+    assert abs(square.st_crossings - square.st) <= 0.01 * abs(square.st), square
+    assert abs(square.cl_mean) < 0.02, square
+    assert rounded.cd_mean < 0.97 * square.cd_mean, (rounded, square)
+    assert rounded.st > 1.02 * square.st, (rounded, square)
