@@ -296,6 +296,13 @@ int vl_batch_macros_field(vl_batch* b, int k, double* rho, double* ux, double* u
  * equilibria of the FP64 fields rho, ux, uy (n = nx * ny values each, row-major) into both
  * population buffers, solids at rest. The warm-start hook of the batched engine. */
 int vl_batch_init(vl_batch* b, int k, const double* rho, const double* ux, const double* uy);
+/* The same from a coarse cell-centred grid of normalised fields in device memory (FP32
+ * [gh][gw][gc], gc >= 3): lattice cell (x, y) samples it bilinearly at column (x - x0) / dx - 1/2
+ * and row (y - y0) / dy - 1/2, clamped at the grid's edges, and decodes channels 0-2 to
+ * u_x = u (1 + v0), u_y = u v1, rho = 1 + 1.5 u^2 v2 (the warm-start network's output), all on the
+ * device. */
+int vl_batch_init_grid(vl_batch* b, int k, const float* grid, int gh, int gw, int gc, double x0, double dx, double y0,
+                       double dy, double u);
 int vl_batch_flags(vl_batch* b, int k, uint8_t* out);
 int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
 

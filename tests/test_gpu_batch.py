@@ -154,3 +154,36 @@ def test_batch_set_steps_matches_a_shorter_run(gpu):
     for k in range(len(cases)):
         assert b.state_hash(k) == ref.state_hash(k), k
         assert np.array_equal(b.force_history(k), ref.force_history(k)), k
+
+
+def test_batch_init_from_a_grid_matches_the_host_decode(gpu):
+    """vl_batch_init_grid (bilinear sampling and decoding of a coarse grid of normalised fields on
+    the device) gives the fields of the host decode followed by vl_batch_init."""
+    V = gpu
+    import torch
+    from vortexlab_b200 import warmstart as WS
+    from vortexlab_b200.batch import Batch
+    cases = _cases(V)
+    rng = np.random.default_rng(4)
+    grids = [(0.2 * rng.standard_normal((WS.H, WS.W, 8))).astype(np.float32) for _ in cases]
+    out = []
+    for device in (False, True):
+        b = Batch("f64")
+        for c in cases:
+            b.add(c.tunnel.spec_warm(c.body), 5)
+        b.build()
+        for k, (c, g) in enumerate(zip(cases, grids)):
+            tn = c.tunnel
+            i = b.info(k)
+            if device:
+                gt = torch.from_numpy(g).cuda()
+                rc = V.lib.vl_batch_init_grid(b._h, k, V._lib.C.c_void_p(gt.data_ptr()), WS.H, WS.W, 8, 0.5,
+                                              20.0 * tn.d / WS.W, 0.5, 10.0 * tn.d / WS.H, tn.u)
+                assert rc == 0, V._lib.last_error()
+            else:
+                b.init(k, *WS.decode_to_lattice(g, i["nx"], i["ny"], tn.d, tn.u))
+        out.append([b.macros_field(k) for k in range(len(cases))])
+        b.close()
+    for host, dev in zip(*out):
+        for a, d in zip(host, dev):
+            assert np.max(np.abs(a - d)) <= 1e-12

@@ -140,6 +140,7 @@ def _declare(L):
         "vl_batch_force_history": (i, [vp, i, P(d), P(u64)]),
         "vl_batch_download": (i, [vp, i, P(d)]),
         "vl_batch_init": (i, [vp, i, P(d), P(d), P(d)]),
+        "vl_batch_init_grid": (i, [vp, i, vp, i, i, i, d, d, d, d, d]),
         "vl_batch_set_steps": (i, [vp, i, C.c_uint64]),
         "vl_batch_macros_field": (i, [vp, i, P(d), P(d), P(d)]),
         "vl_batch_flags": (i, [vp, i, P(C.c_uint8)]),

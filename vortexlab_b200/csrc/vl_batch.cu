@@ -583,6 +583,21 @@ int vl_batch_init(vl_batch* b, int k, const double* rho, const double* ux, const
   return VL_OK;
 }
 
+int vl_batch_init_grid(vl_batch* b, int k, const float* grid, int gh, int gw, int gc, double x0, double dx, double y0,
+                       double dy, double u) {
+  if (!b || !b->built || !grid || k < 0 || (size_t)k >= b->tun.size() || gh < 2 || gw < 2 || gc < 3 || !(dx > 0.0) ||
+      !(dy > 0.0))
+    return fail(VL_EINVAL, "bad arguments");
+  if (b->s != 0) return fail(VL_EINVAL, "a tunnel can only be initialised before the batch's first step");
+  const vl::BatchTunnel& T = b->tun[k];
+  const size_t n = b->plans[k].dom.n;
+  cudaError_t e = b->L->init_grid(T.nx, (int)n, T.ns, b->d_flag + T.cell_off, grid, gh, gw, gc, x0, dx, y0, dy, u,
+                                  b->tunnel_ptr(b->buf[0], k), b->tunnel_ptr(b->buf[1], k), b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "batch init from grid");
+  return VL_OK;
+}
+
 int vl_batch_flags(vl_batch* b, int k, uint8_t* out) {
   if (!b || !out || k < 0 || (size_t)k >= b->plans.size()) return fail(VL_EINVAL, "bad arguments");
   std::memcpy(out, b->plans[k].dom.flag.data(), b->plans[k].dom.n);

@@ -565,6 +565,43 @@ __global__ void k_init(int n, unsigned ns, const uint8_t* __restrict__ flag, con
   }
 }
 
+// Sim::init from fields given on a coarse grid of normalised values (the warm-start network's
+// output, FP32 [gh][gw][gc], device memory): lattice cell (x, y) samples the grid bilinearly at
+// column (x - x0) / dx - 1/2 and row (y - y0) / dy - 1/2 (cell-centred grid, clamped at its edges),
+// and channels 0-2 decode to u_x = u (1 + v0), u_y = u v1, rho = 1 + 1.5 u^2 v2; solids get
+// (1, 0, 0). The equilibria go into both buffers.
+template <class S>
+__global__ void k_init_grid(int nx, int n, unsigned ns, const uint8_t* __restrict__ flag, const float* __restrict__ g,
+                            int gh, int gw, int gc, double x0, double dx, double y0, double dy, double u,
+                            S* __restrict__ a, S* __restrict__ b) {
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += gridDim.x * blockDim.x) {
+    double r = 1.0, vx = 0.0, vy = 0.0;
+    if (flag[idx] != 2) {
+      const int x = idx % nx, y = idx / nx;
+      const double gx = ((double)x - x0) / dx - 0.5, gy = ((double)y - y0) / dy - 0.5;
+      const int ix = min(max((int)floor(gx), 0), gw - 2), iy = min(max((int)floor(gy), 0), gh - 2);
+      const double fx = fmin(fmax(gx - ix, 0.0), 1.0), fy = fmin(fmax(gy - iy, 0.0), 1.0);
+      double v[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        const float* p = g + ((size_t)iy * gw + ix) * gc + c;
+        const double f00 = p[0], f01 = p[gc], f10 = p[(size_t)gw * gc], f11 = p[(size_t)gw * gc + gc];
+        v[c] = (1.0 - fy) * ((1.0 - fx) * f00 + fx * f01) + fy * ((1.0 - fx) * f10 + fx * f11);
+      }
+      vx = u * (1.0 + v[0]);
+      vy = u * v[1];
+      r = 1.0 + 1.5 * u * u * v[2];
+    }
+    double feq[9];
+    equilibrium(r, vx, vy, feq);
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      Store<S>::st(a + (size_t)i * ns + idx, i, (typename Store<S>::R)feq[i]);
+      Store<S>::st(b + (size_t)i * ns + idx, i, (typename Store<S>::R)feq[i]);
+    }
+  }
+}
+
 // Populations to FP64 in the reference layout (plane stride n).
 template <class S>
 __global__ void k_to_f64(int n, unsigned ns, const S* __restrict__ a, double* __restrict__ out) {

@@ -18,6 +18,9 @@ struct Launchers {
   cudaError_t (*step)(const StepParams& p, int ck, const void* a, void* b, cudaStream_t s);
   cudaError_t (*init)(int n, unsigned ns, const uint8_t* flag, const double* rho, const double* ux,
                       const double* uy, double rho0, double ux0, double uy0, void* a, void* b, cudaStream_t s);
+  // Init from a coarse grid of normalised fields (k_init_grid).
+  cudaError_t (*init_grid)(int nx, int n, unsigned ns, const uint8_t* flag, const float* g, int gh, int gw, int gc,
+                           double x0, double dx, double y0, double dy, double u, void* a, void* b, cudaStream_t s);
   cudaError_t (*to_f64)(int n, unsigned ns, const void* a, double* out, cudaStream_t s);
   cudaError_t (*from_f64)(int n, unsigned ns, const double* in, void* a, cudaStream_t s);
   cudaError_t (*macros)(int n, unsigned ns, const uint8_t* flag, double gx, double gy, const void* a,

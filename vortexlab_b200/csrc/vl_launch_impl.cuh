@@ -35,6 +35,11 @@ struct LaunchImpl {
     k_init<S><<<grid_for(n), 256, 0, s>>>(n, ns, flag, rho, ux, uy, rho0, ux0, uy0, (S*)a, (S*)b);
     return cudaGetLastError();
   }
+  static cudaError_t init_grid(int nx, int n, unsigned ns, const uint8_t* flag, const float* g, int gh, int gw, int gc,
+                               double x0, double dx, double y0, double dy, double u, void* a, void* b, cudaStream_t s) {
+    k_init_grid<S><<<grid_for(n), 256, 0, s>>>(nx, n, ns, flag, g, gh, gw, gc, x0, dx, y0, dy, u, (S*)a, (S*)b);
+    return cudaGetLastError();
+  }
   static cudaError_t to_f64(int n, unsigned ns, const void* a, double* out, cudaStream_t s) {
     k_to_f64<S><<<grid_for(n), 256, 0, s>>>(n, ns, (const S*)a, out);
     return cudaGetLastError();
@@ -69,7 +74,7 @@ struct LaunchImpl {
     return cudaGetLastError();
   }
   static const Launchers& table() {
-    static const Launchers t = {sizeof(S), &step, &init, &to_f64, &from_f64, &macros, &reduce, &gather, &probe, &batch_step};
+    static const Launchers t = {sizeof(S), &step, &init, &init_grid, &to_f64, &from_f64, &macros, &reduce, &gather, &probe, &batch_step};
     return t;
   }
 };

@@ -10,9 +10,10 @@ level, and applies two 3x3 convolutions; a 1x1 convolution gives the output. Wit
 c0 = 32 it has 1.95 M parameters.
 
 Every convolution is an im2col gather plus a BF16 GEMM on the tcgen05 tensor cores with FP32
-accumulation (vl_nn_gemm_bf16); its backward pass is two more GEMMs (weights: dz^T cols; data:
-dz W, then col2im). Master weights and Adam moments are FP32. torch provides device memory only:
-every arithmetic operation on the device runs in this library's kernels.
+accumulation (vl_nn_gemm_bf16); its backward pass is two more GEMMs (weights: cols^T dz; data: the
+im2col of dz times the mirrored weights for stride-1 layers, dz W^T then col2im for stride 2).
+Master weights and Adam moments are FP32. torch provides device memory only: every arithmetic
+operation on the device runs in this library's kernels.
 
 Inputs (4 channels): body mask, (Re - 125) / 75, x and y in [-1, 1]. Targets / outputs (the first
 3 of COUT channels): u_x / u - 1, u_y / u, 2 (rho - 1) / (3 u^2).
@@ -613,19 +614,33 @@ def masked_mse(pred, data: Dataset):
 # ---------------------------------------------------------------------------- warm-started runs
 def warm_batch(net, cases, precision="f32", batch=16):
     """A built batch of the cases in their warm form (no ramp, no twist), every tunnel initialised
-    from the network's prediction. Returns (batch, seconds spent on inference and initialisation)."""
+    from the network's prediction: inputs encoded on the host from the tunnels' flags, the network
+    and the decode to lattice fields (vl_batch_init_grid) on the device. Returns (batch, seconds
+    spent on encoding, inference and initialisation)."""
     from .batch import Batch
+    torch = _t()
     b = Batch(precision)
     for c in cases:
         b.add(c.tunnel.spec_warm(c.body), c.steps)
     b.build()
     t0 = time.perf_counter()
     x = np.stack([encode_input(b.flags(k), c.tunnel.d, c.tunnel.re) for k, c in enumerate(cases)])
-    pred = predict(net, x, batch)
-    for k, c in enumerate(cases):
-        i = b.info(k)
-        rho, ux, uy = decode_to_lattice(pred[k], i["nx"], i["ny"], c.tunnel.d, c.tunnel.u)
-        b.init(k, rho, ux, uy)
+    if net.B != batch:
+        net.alloc(batch)
+    X = bf16_upload(x)
+    xb = torch.zeros(batch, H, W, CIN, dtype=torch.bfloat16, device="cuda")
+    per = H * W * net.cout
+    for i in range(0, len(cases), batch):
+        m = min(batch, len(cases) - i)
+        xb.zero_()
+        xb[:m].copy_(X[i:i + m])
+        y = net.forward(xb)
+        torch.cuda.synchronize()
+        for j in range(m):
+            tn = cases[i + j].tunnel
+            check(lib.vl_batch_init_grid(b._h, i + j, C.c_void_p(y.data_ptr() + 4 * j * per), H, W, net.cout,
+                                         0.5, 20.0 * tn.d / W, 0.5, 10.0 * tn.d / H, tn.u))
+    net.check_errors()
     return b, time.perf_counter() - t0
 
 
@@ -669,19 +684,38 @@ def study(n_train=2000, n_test=200, gen_units=50.0, eval_units=100.0, train_seco
     return out
 
 
+def compare(n_test=200, eval_units=100.0, log=print):
+    """The time-to-converged comparison of `study` with the shipped network (no training)."""
+    from . import convergence as CV
+    from .batch import seeded_tunnels
+    test = seeded_tunnels(seed=TEST_SEED, count=n_test, units=eval_units)
+    t0 = time.perf_counter()
+    out = CV.warm_comparison(load_pretrained(), test)
+    log(f"comparison in {time.perf_counter() - t0:.1f} s: {out['summary']}")
+    return dict(config=dict(n_test=n_test, eval_units=eval_units, network=PRETRAINED), comparison=out)
+
+
 if __name__ == "__main__":
     # python -m vortexlab_b200.warmstart OUTDIR [n_train n_test gen_units eval_units train_seconds epochs]
+    # python -m vortexlab_b200.warmstart compare OUTDIR [n_test eval_units]   (the shipped network)
     import json
-    import os
     import sys
-    outdir = sys.argv[1]
-    os.makedirs(outdir, exist_ok=True)
-    names = ["n_train", "n_test", "gen_units", "eval_units", "train_seconds", "epochs"]
-    kw = {k: (int(v) if k.startswith("n_") or k == "epochs" else float(v)) for k, v in zip(names, sys.argv[2:])}
 
     def log(m):
         print(m, flush=True)
 
+    if sys.argv[1] == "compare":
+        outdir = sys.argv[2]
+        os.makedirs(outdir, exist_ok=True)
+        args = sys.argv[3:]
+        res = compare(int(args[0]) if args else 200, float(args[1]) if len(args) > 1 else 100.0, log=log)
+        with open(os.path.join(outdir, "warmstart_compare.json"), "w") as f:
+            json.dump(res, f, default=float, indent=1)
+        sys.exit(0)
+    outdir = sys.argv[1]
+    os.makedirs(outdir, exist_ok=True)
+    names = ["n_train", "n_test", "gen_units", "eval_units", "train_seconds", "epochs"]
+    kw = {k: (int(v) if k.startswith("n_") or k == "epochs" else float(v)) for k, v in zip(names, sys.argv[2:])}
     res = study(**kw, log=log, weights_out=os.path.join(outdir, "warmstart_unet.npz"))
     with open(os.path.join(outdir, "warmstart_study.json"), "w") as f:
         json.dump(res, f, default=float, indent=1)
