@@ -310,10 +310,13 @@ int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
  * No reference counterpart. Device-pointer kernels of the warm-start network (a convolutional
  * network trained on solver-generated wakes); the caller owns every buffer.
  * vl_nn_gemm_bf16: out[m, n] = epilogue(sum_k a[m, k] * b[n, k]) on the tcgen05 tensor cores,
- * BF16 inputs (row-major, K contiguous, leading dimensions lda / ldb multiples of 8), FP32
- * accumulation. flags: 1 accumulate into FP32 out, 2 add bias[n], 4 ReLU, 8 store BF16.
- * bn: tile width 32, 64, 128 or 256. err (device int, may be NULL) becomes nonzero if a tile
- * timed out waiting for its data. Asynchronous on `stream`. */
+ * BF16 inputs (leading dimensions lda / ldb multiples of 8), FP32 accumulation. By default a is
+ * stored [M][K] and b [N][K] (K contiguous); with VL_GEMM_A_MN a is stored [K][M] and with
+ * VL_GEMM_B_MN b is stored [K][N] (M or N contiguous; then bn >= 64). flags also select the
+ * epilogue: 1 accumulate into FP32 out, 2 add bias[n], 4 ReLU, 8 store BF16. bn: tile width 32,
+ * 64, 128 or 256. err (device int, may be NULL) becomes nonzero if a tile timed out waiting for
+ * its data. Asynchronous on `stream`. */
+enum { VL_GEMM_ACCUM = 1, VL_GEMM_BIAS = 2, VL_GEMM_RELU = 4, VL_GEMM_BF16 = 8, VL_GEMM_A_MN = 16, VL_GEMM_B_MN = 32 };
 int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N, int K, void* out, int ldc,
                     const float* bias, int flags, int bn, int* err, void* stream);
 /* Gathers and elementwise kernels around the GEMM. Activations are NHWC BF16 (row = pixel,
@@ -322,7 +325,7 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
 int vl_nn_im2col(const void* x, int B, int H, int W, int C, int stride, int kp, void* cols, void* stream);
 int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int kp, float* dx, int accumulate,
                  void* stream);
-/* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and transposed [C, R]; colsum (may be NULL)
+/* dz = dy * (y > 0) (relu) or dy, as BF16 [R, C] and (dzt, may be NULL) transposed [C, R]; colsum (may be NULL)
  * receives per 32-row tile column sums [C][ceil(R / 32)] that vl_nn_bias_grad reduces to db. */
 int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, float* colsum,
                   void* stream);

@@ -80,3 +80,30 @@ def test_gemm_split_k_accumulates(gpu):
     again2 = torch.zeros(M, N, dtype=torch.float32, device="cuda")
     _gemm(V, a.cuda(), b.cuda(), again2, bn=128)
     assert torch.equal(again, again2)
+
+
+@pytest.mark.parametrize("layout", ["mn_k", "k_mn", "mn_mn"])
+@pytest.mark.parametrize("M,N,K,bn", [(256, 64, 128, 64), (200, 96, 1000, 128), (640, 32, 4096, 64),
+                                      (136, 256, 72, 256)])
+def test_gemm_mn_major_operands(gpu, layout, M, N, K, bn):
+    """Operands stored transposed (MN-major: A as [K][M], B as [K][N]) give the same product."""
+    V = gpu
+    import torch
+    g = torch.Generator().manual_seed(M + 3 * N + 7 * K)
+    a = torch.randn(M, K, generator=g).bfloat16()
+    b = torch.randn(N, K, generator=g).bfloat16()
+    ref = a.double() @ b.double().T
+    a_mn, b_mn = layout.startswith("mn"), layout.endswith("_mn")
+    ad = (a.T.contiguous() if a_mn else a).cuda()
+    bd = (b.T.contiguous() if b_mn else b).cuda()
+    out = torch.zeros(M, N, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    flags = (16 if a_mn else 0) | (32 if b_mn else 0)
+    rc = V.lib.vl_nn_gemm_bf16(C.c_void_p(ad.data_ptr()), M if a_mn else K, C.c_void_p(bd.data_ptr()),
+                               N if b_mn else K, M, N, K, C.c_void_p(out.data_ptr()), N, None, flags, bn,
+                               C.cast(C.c_void_p(err.data_ptr()), C.POINTER(C.c_int)), None)
+    assert rc == 0, V._lib.last_error()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    got = out.cpu().double()
+    assert torch.max(torch.abs(got - ref)).item() <= 1e-4 * max(1.0, torch.max(torch.abs(ref)).item()) * (K ** 0.5)

@@ -96,11 +96,38 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
   return d;
 }
 
-// Instruction descriptor: BF16 x BF16 -> FP32, both K-major, M = 128, N = bn.
-__host__ __device__ constexpr uint32_t instr_desc_bf16(int bn) {
+// Shared-memory matrix descriptor of an MN-major tile with 128-byte swizzle: each K row holds 64
+// consecutive M (or N) values (128 bytes), 8 K rows form a 1024-byte swizzle atom; consecutive
+// atoms along K are 1024 bytes apart (stride byte offset) and consecutive 64-wide column blocks
+// along M / N are 64 K rows = 8192 bytes apart (leading byte offset).
+#ifndef VL_MN_LBO
+#define VL_MN_LBO 8192u
+#endif
+#ifndef VL_MN_SBO
+#define VL_MN_SBO 1024u
+#endif
+__device__ __forceinline__ uint64_t smem_desc_sw128_mn(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((VL_MN_LBO >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((VL_MN_SBO >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  d |= (uint64_t)2u << 61;
+  return d;
+}
+
+// Operand layouts (kernel argument `op`): bit 0 A is MN-major (stored [K][M]), bit 1 B is
+// MN-major (stored [K][N]); otherwise K-major ([M][K], [N][K]).
+enum : int { OP_A_MN = 1, OP_B_MN = 2 };
+
+// Instruction descriptor: BF16 x BF16 -> FP32, M = 128, N = bn, A / B transposed (MN-major) on
+// request.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int bn, int op = 0) {
   return (1u << 4)                      // D format FP32
          | (1u << 7)                    // A format BF16
          | (1u << 10)                   // B format BF16
+         | ((op & OP_A_MN) ? (1u << 15) : 0u)  // A MN-major
+         | ((op & OP_B_MN) ? (1u << 16) : 0u)  // B MN-major
          | ((uint32_t)(bn >> 3) << 17)  // N >> 3
          | ((uint32_t)(BM >> 4) << 24); // M >> 4
 }
@@ -108,7 +135,7 @@ __host__ __device__ constexpr uint32_t instr_desc_bf16(int bn) {
 template <int BN>
 __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CUtensorMap tmA,
                                                       const __grid_constant__ CUtensorMap tmB, int kblocks_total,
-                                                      int kb_per, int stages, EpiParams ep) {
+                                                      int kb_per, int stages, int op, EpiParams ep) {
   static_assert(BN == 32 || BN == 64 || BN == 128 || BN == 256, "tile N");
   constexpr int A_BYTES = BM * BK * 2;
   constexpr int B_BYTES = BN * BK * 2;
@@ -154,8 +181,19 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
       if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) { atomicExch(&failed, 1); break; }
       uint8_t* sa = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
-      tma_load_2d(&tmA, &full[s], sa, (kb_first + kb) * BK, m0);
-      tma_load_2d(&tmB, &full[s], sa + A_BYTES, (kb_first + kb) * BK, n0);
+      const int k0 = (kb_first + kb) * BK;
+      if (op & OP_A_MN) {        // two 64-row K x 64-column M boxes
+        tma_load_2d(&tmA, &full[s], sa, m0, k0);
+        tma_load_2d(&tmA, &full[s], sa + 8192, m0 + 64, k0);
+      } else {
+        tma_load_2d(&tmA, &full[s], sa, k0, m0);
+      }
+      if (op & OP_B_MN) {        // BN / 64 boxes of 64 K rows x 64 N columns
+#pragma unroll
+        for (int c = 0; c < BN / 64; ++c) tma_load_2d(&tmB, &full[s], sa + A_BYTES + 8192 * c, n0 + 64 * c, k0);
+      } else {
+        tma_load_2d(&tmB, &full[s], sa + A_BYTES, k0, n0);
+      }
       issued = kb + 1;
     }
     if (failed) {
@@ -165,7 +203,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer.
-    constexpr uint32_t idesc = instr_desc_bf16(BN);
+    const uint32_t idesc = instr_desc_bf16(BN, op);
     bool ok = true;
     for (int kb = 0; kb < kblocks && ok; ++kb) {
       const int s = kb % stages;
@@ -176,9 +214,10 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
       const uint32_t b_addr = a_addr + A_BYTES;
 #pragma unroll
       for (int k = 0; k < BK / 16; ++k) {
-        // 16 BF16 = 32 bytes further along K inside the 128-byte swizzle row
-        const uint64_t da = smem_desc_sw128(a_addr + 32u * k);
-        const uint64_t db = smem_desc_sw128(b_addr + 32u * k);
+        // K-major: 16 BF16 = 32 bytes further along K inside the 128-byte swizzle row;
+        // MN-major: 16 K rows of 128 bytes further
+        const uint64_t da = (op & OP_A_MN) ? smem_desc_sw128_mn(a_addr + 2048u * k) : smem_desc_sw128(a_addr + 32u * k);
+        const uint64_t db = (op & OP_B_MN) ? smem_desc_sw128_mn(b_addr + 2048u * k) : smem_desc_sw128(b_addr + 32u * k);
         const uint32_t accumulate = (kb > 0 || k > 0) ? 1u : 0u;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"

@@ -95,8 +95,8 @@ __global__ void k_split_reduce(const float* __restrict__ ws, int splits, int M, 
 }
 
 template <int BN>
-int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int K, const vl::gemm::EpiParams& ep,
-                cudaStream_t s) {
+int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int K, int op,
+                const vl::gemm::EpiParams& ep, cudaStream_t s) {
   static bool configured[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -137,7 +137,7 @@ int launch_gemm(const CUtensorMap& ta, const CUtensorMap& tb, int M, int N, int 
   // epilogue overlaps the next one's loads. TMEM stays within its 512 columns in both cases.
   const int stages = kb_per <= 8 ? 2 : vl::gemm::STAGES;
   dim3 grid(gx, gy, splits);
-  vl::gemm::k_gemm_bf16<BN><<<grid, 128, vl::gemm::smem_bytes<BN>(stages), s>>>(ta, tb, kblocks, kb_per, stages, p);
+  vl::gemm::k_gemm_bf16<BN><<<grid, 128, vl::gemm::smem_bytes<BN>(stages), s>>>(ta, tb, kblocks, kb_per, stages, op, p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(VL_ECUDA, std::string("gemm launch: ") + cudaGetErrorString(e));
   if (splits > 1) {
@@ -159,10 +159,13 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
   if (!a || !b || !out || M <= 0 || N <= 0 || K <= 0) return fail(VL_EINVAL, "gemm: bad arguments");
   if (bn != 32 && bn != 64 && bn != 128 && bn != 256) return fail(VL_EINVAL, "gemm: tile N must be 32, 64, 128 or 256");
   if ((flags & vl::gemm::EPI_BIAS) && !bias) return fail(VL_EINVAL, "gemm: bias requested without a bias");
+  const int op = ((flags & VL_GEMM_A_MN) ? vl::gemm::OP_A_MN : 0) | ((flags & VL_GEMM_B_MN) ? vl::gemm::OP_B_MN : 0);
+  if ((op & vl::gemm::OP_B_MN) && bn < 64) return fail(VL_EINVAL, "gemm: an MN-major B needs a tile N of 64 or more");
   CUtensorMap ta, tb;
-  int rc = make_map(&ta, a, (uint64_t)M, (uint64_t)K, (uint64_t)lda, vl::gemm::BM);
+  const bool amn = op & vl::gemm::OP_A_MN, bmn = op & vl::gemm::OP_B_MN;
+  int rc = make_map(&ta, a, (uint64_t)(amn ? K : M), (uint64_t)(amn ? M : K), (uint64_t)lda, amn ? 64u : vl::gemm::BM);
   if (rc) return rc;
-  rc = make_map(&tb, b, (uint64_t)N, (uint64_t)K, (uint64_t)ldb, (uint32_t)bn);
+  rc = make_map(&tb, b, (uint64_t)(bmn ? K : N), (uint64_t)(bmn ? N : K), (uint64_t)ldb, bmn ? 64u : (uint32_t)bn);
   if (rc) return rc;
   vl::gemm::EpiParams ep;
   ep.out = out;
@@ -170,14 +173,14 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
   ep.bias = bias;
   ep.m_valid = M;
   ep.n_valid = N;
-  ep.flags = flags;
+  ep.flags = flags & (vl::gemm::EPI_ACCUM | vl::gemm::EPI_BIAS | vl::gemm::EPI_RELU | vl::gemm::EPI_BF16);
   ep.err = err;
   cudaStream_t s = (cudaStream_t)stream;
   switch (bn) {
-    case 32: return launch_gemm<32>(ta, tb, M, N, K, ep, s);
-    case 64: return launch_gemm<64>(ta, tb, M, N, K, ep, s);
-    case 128: return launch_gemm<128>(ta, tb, M, N, K, ep, s);
-    default: return launch_gemm<256>(ta, tb, M, N, K, ep, s);
+    case 32: return launch_gemm<32>(ta, tb, M, N, K, op, ep, s);
+    case 64: return launch_gemm<64>(ta, tb, M, N, K, op, ep, s);
+    case 128: return launch_gemm<128>(ta, tb, M, N, K, op, ep, s);
+    default: return launch_gemm<256>(ta, tb, M, N, K, op, ep, s);
   }
 }
 
@@ -290,7 +293,7 @@ __global__ void k_act_bwd(const float* __restrict__ dy, const bf16* __restrict__
   for (int j = threadIdx.y; j < 32; j += blockDim.y) {
     const int c = c0 + j, r = r0 + threadIdx.x;
     const float v = tile[threadIdx.x][j];
-    if (c < C && r < R) dzt[(long long)c * R + r] = __float2bfloat16_rn(v);
+    if (dzt && c < C && r < R) dzt[(long long)c * R + r] = __float2bfloat16_rn(v);
     float sum = v;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -479,7 +482,7 @@ int vl_nn_col2im(const float* dcols, int B, int H, int W, int C, int stride, int
 
 int vl_nn_act_bwd(const float* dy, const void* y, int R, int C, int relu, void* dz, void* dzt, float* colsum,
                   void* stream) {
-  if (!dy || !dz || !dzt || (relu && !y)) return fail(VL_EINVAL, "act_bwd: bad arguments");
+  if (!dy || !dz || (relu && !y)) return fail(VL_EINVAL, "act_bwd: bad arguments");
   dim3 grid((C + 31) / 32, (R + 31) / 32), block(32, 8);
   k_act_bwd<<<grid, block, 0, (cudaStream_t)stream>>>(dy, (const bf16*)y, R, C, relu, (bf16*)dz, (bf16*)dzt, colsum,
                                                       (R + 31) / 32);

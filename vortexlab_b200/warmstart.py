@@ -10,8 +10,9 @@ level, and applies two 3x3 convolutions; a 1x1 convolution gives the output. Wit
 c0 = 32 it has 1.95 M parameters.
 
 Every convolution is an im2col gather plus a BF16 GEMM on the tcgen05 tensor cores with FP32
-accumulation (vl_nn_gemm_bf16); its backward pass is two more GEMMs (weights: cols^T dz; data: the
-im2col of dz times the mirrored weights for stride-1 layers, dz W^T then col2im for stride 2).
+accumulation (vl_nn_gemm_bf16); its backward pass is two more GEMMs (weights: cols^T dz, with both
+operands read MN-major where they lie, no transposes; data: the im2col of dz times the mirrored
+weights for stride-1 layers, dz W^T then col2im for stride 2).
 Master weights and Adam moments are FP32. torch provides device memory only: every arithmetic
 operation on the device runs in this library's kernels.
 
@@ -73,9 +74,14 @@ class _Err:
         return C.cast(C.c_void_p(self.t.data_ptr()), C.POINTER(C.c_int))
 
 
+A_MN, B_MN = 16, 32   # operand stored [K][M] / [K][N] (MN-major) instead of [M][K] / [N][K]
+
+
 def gemm(a, lda, b, ldb, M, N, K, out, ldc, flags=0, bias=None, err=None):
-    """out = epilogue(a[M, K] b[N, K]^T) on the tensor cores (all device tensors)."""
-    check(lib.vl_nn_gemm_bf16(_p(a), lda, _p(b), ldb, M, N, K, _p(out), ldc, _fp(bias), flags, _bn(N),
+    """out = epilogue(A B^T) on the tensor cores (all device tensors); A is a[M, K] (or a[K, M]
+    with A_MN), B is b[N, K] (or b[K, N] with B_MN)."""
+    bn = max(64, _bn(N)) if flags & B_MN else _bn(N)
+    check(lib.vl_nn_gemm_bf16(_p(a), lda, _p(b), ldb, M, N, K, _p(out), ldc, _fp(bias), flags, bn,
                               err.ptr() if err is not None else None, None))
 
 
@@ -130,7 +136,6 @@ class Conv:
         self.rows = B * self.ho * self.wo
         bf = dict(dtype=torch.bfloat16, device="cuda")
         self.cols = torch.zeros(self.rows, self.kp, **bf) if self.k == 3 else None
-        self.colst = torch.zeros(self.kp, self.rows, **bf)
         self.flip = self.k == 3 and self.stride == 1
         if self.flip:       # input gradient as a convolution of dz with mirrored weights
             self.kpf = _kp(9 * self.cout)
@@ -141,7 +146,6 @@ class Conv:
         self.y = torch.zeros(self.rows, self.cout, **bf) if self.relu else \
             torch.zeros(self.rows, self.cout, dtype=torch.float32, device="cuda")
         self.dz = torch.zeros(self.rows, self.cout, **bf)
-        self.dzt = torch.zeros(self.cout, self.rows, **bf)
         self.colsum = torch.zeros(self.cout, (self.rows + 31) // 32, dtype=torch.float32, device="cuda")
 
     def forward(self, x, err):
@@ -160,11 +164,11 @@ class Conv:
         """dy: FP32 [rows, cout], the gradient of the layer output. Writes (or, with `accumulate`,
         adds) the input gradient into dx (FP32 [B, h, w, cin]); sets gw and gb."""
         check(lib.vl_nn_act_bwd(_p(dy), _p(self.y) if self.relu else None, self.rows, self.cout, int(self.relu),
-                                _p(self.dz), _p(self.dzt), _p(self.colsum), None))
+                                _p(self.dz), None, _p(self.colsum), None))
         check(lib.vl_nn_bias_grad(_p(self.colsum), self.rows, self.cout, _p(self.gb), None))
+        # weight gradient gw^T [kp, cout] = cols^T dz: both operands read MN-major as they lie
         a = self.cols if self.k == 3 else self.x
-        check(lib.vl_nn_transpose_bf16(_p(a), self.rows, self.kp, _p(self.colst), None))
-        gemm(self.colst, self.rows, self.dzt, self.rows, self.kp, self.cout, self.rows, self.gwt, self.cout, 0, None, err)
+        gemm(a, self.kp, self.dz, self.cout, self.kp, self.cout, self.rows, self.gwt, self.cout, A_MN | B_MN, None, err)
         if not need_dx:
             return
         if self.flip:
