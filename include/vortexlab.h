@@ -35,7 +35,10 @@ extern "C" {
 #define VL_OK 0
 #define VL_EINVAL (-1)       /* contract violation (the reference panics)                      */
 #define VL_ECUDA (-2)        /* CUDA runtime error or no CUDA device                           */
-#define VL_EDIVERGED (-3)    /* non-finite force: src/cases/cylinder.rs:179-186, tunnel.rs:78-84 */
+#define VL_EDIVERGED (-3)    /* non-finite force: src/cases/cylinder.rs:179-186, tunnel.rs:78-84.
+                              * The step functions, like Sim::step, do not fail on divergence: they
+                              * record it on the device (vl_sim_status, vl_batch_status), and the
+                              * case drivers raise this code, as the reference's cases return Err. */
 #define VL_ENOMEM (-4)       /* device or host allocation failed                               */
 #define VL_EUNSUPPORTED (-5) /* valid request that this build does not implement               */
 
