@@ -318,8 +318,12 @@ int vl_batch_state_hash(vl_batch* b, int k, uint64_t* out);
  * VL_GEMM_B_MN b is stored [K][N] (M or N contiguous; then bn >= 64). flags also select the
  * epilogue: 1 accumulate into FP32 out, 2 add bias[n], 4 ReLU, 8 store BF16. bn: tile width 32,
  * 64, 128 or 256. err (device int, may be NULL) becomes nonzero if a tile timed out waiting for
- * its data. Asynchronous on `stream`. */
-enum { VL_GEMM_ACCUM = 1, VL_GEMM_BIAS = 2, VL_GEMM_RELU = 4, VL_GEMM_BF16 = 8, VL_GEMM_A_MN = 16, VL_GEMM_B_MN = 32 };
+ * its data (every wait of the kernel is bounded; the tile is then skipped and its tensor memory
+ * freed). VL_GEMM_TEST_TIMEOUT exercises that path: the first operand load of every tile is never
+ * issued and the waits give up after a short limit; out is not written, err is set. Asynchronous
+ * on `stream`. */
+enum { VL_GEMM_ACCUM = 1, VL_GEMM_BIAS = 2, VL_GEMM_RELU = 4, VL_GEMM_BF16 = 8, VL_GEMM_A_MN = 16, VL_GEMM_B_MN = 32,
+       VL_GEMM_TEST_TIMEOUT = 64 };
 int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N, int K, void* out, int ldc,
                     const float* bias, int flags, int bn, int* err, void* stream);
 /* Gathers and elementwise kernels around the GEMM. Activations are NHWC BF16 (row = pixel,

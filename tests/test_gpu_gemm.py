@@ -107,3 +107,27 @@ def test_gemm_mn_major_operands(gpu, layout, M, N, K, bn):
     assert int(err.item()) == 0
     got = out.cpu().double()
     assert torch.max(torch.abs(got - ref)).item() <= 1e-4 * max(1.0, torch.max(torch.abs(ref)).item()) * (K ** 0.5)
+
+
+def test_gemm_wait_that_runs_out_reports_and_leaves_the_context_usable(gpu):
+    """Failure detection without a fault: with the test hook the first operand load of every tile
+    is never issued, so the tile's bounded waits run out; the kernel skips the tile, frees its
+    tensor memory and sets the error word, and the next GEMM on the same context is correct."""
+    V = gpu
+    import torch
+    g = torch.Generator().manual_seed(12)
+    M, N, K = 256, 64, 256
+    a = torch.randn(M, K, generator=g).bfloat16().cuda()
+    b = torch.randn(N, K, generator=g).bfloat16().cuda()
+    out = torch.full((M, N), 7.0, dtype=torch.float32, device="cuda")
+    err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rc = V.lib.vl_nn_gemm_bf16(C.c_void_p(a.data_ptr()), K, C.c_void_p(b.data_ptr()), K, M, N, K,
+                               C.c_void_p(out.data_ptr()), N, None, 64, 64,
+                               C.cast(C.c_void_p(err.data_ptr()), C.POINTER(C.c_int)), None)
+    assert rc == 0, V._lib.last_error()
+    torch.cuda.synchronize()
+    assert int(err.item()) == 1
+    assert bool(torch.all(out == 7.0))
+    _gemm(V, a, b, out, bn=64)
+    ref = a.cpu().double() @ b.cpu().double().T
+    assert torch.max(torch.abs(out.cpu().double() - ref)).item() <= 1e-4 * torch.max(torch.abs(ref)).item() * K ** 0.5

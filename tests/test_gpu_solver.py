@@ -247,3 +247,39 @@ def test_rounding_the_corners_lowers_drag_and_raises_the_shedding_frequency(gpu)
     assert abs(square.cl_mean) < 0.02, square
     assert rounded.cd_mean < 0.97 * square.cd_mean, (rounded, square)
     assert rounded.st > 1.02 * square.st, (rounded, square)
+
+
+def test_nonfinite_force_is_recorded_on_the_device(gpu):
+    """Failure detection without a GPU fault: NaN populations planted from the host into one
+    boundary node reach the force of the next step; the device records that step (the step
+    functions go on, as Sim::step does, and the case drivers then report divergence)."""
+    d = S.periodic_box(48, 36, collision="bgk")
+    d["kinds"] = [("wall", None, 0, 0, ("circle", 20.3, 15.7, 6.4))]
+    d["paint"] = [("shape", 1)]
+    sim = S.product_sim(d)
+    sim.init((1.0, 0.02, 0.0))
+    sim.step(5)
+    assert sim.status() == (False, 0)
+    f = sim.populations().copy()
+    ys, xs = np.nonzero(sim.flags() == 1)
+    f[:, ys[0], xs[0]] = np.nan
+    sim.set_populations(f)
+    sim.step(3)
+    assert sim.status() == (True, 5)
+    assert not np.all(np.isfinite(sim.force))
+
+
+def test_nonfinite_force_is_recorded_per_tunnel_in_a_batch(gpu):
+    """The same in a batch: a NaN start field in one tunnel is flagged for that tunnel only."""
+    from vortexlab_b200.batch import Batch, seeded_tunnels
+    cases = seeded_tunnels(seed=99, count=3, dmin=8, dmax=14, units=0.5)
+    b = Batch("f32")
+    for c in cases:
+        b.add(c.tunnel.spec_warm(c.body), c.steps)
+    b.build()
+    i = b.info(1)
+    rho = np.ones((i["ny"], i["nx"]))
+    rho[:, :] = np.nan
+    b.init(1, rho, 0.05, 0.0)
+    b.run()
+    assert [b.status(k)[1] for k in range(3)] == [False, True, False]

@@ -44,6 +44,8 @@ struct EpiParams {
   int flags;
   int* err;          // device error word (0 = fine)
   long long split_stride;  // elements between the partial results of consecutive K splits
+  unsigned spin_limit;     // polls of an mbarrier before a wait gives up
+  int drop_load;           // test hook: stage 0's A load is never issued, so every wait on it runs out
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -59,9 +61,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
 }
 
 // Bounded wait for the phase of parity `parity` to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, unsigned limit) {
   const uint32_t addr = smem_u32(bar);
-  for (unsigned it = 0; it < kSpinLimit; ++it) {
+  for (unsigned it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -178,11 +180,13 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     for (int kb = 0; kb < kblocks; ++kb) {
       const int s = kb % stages;
       const uint32_t round = (uint32_t)(kb / stages);
-      if (!mbar_wait(&empty[s], (round & 1u) ^ 1u)) { atomicExch(&failed, 1); break; }
+      if (!mbar_wait(&empty[s], (round & 1u) ^ 1u, ep.spin_limit)) { atomicExch(&failed, 1); break; }
       uint8_t* sa = smem + s * STAGE_BYTES;
       mbar_expect_tx(&full[s], STAGE_BYTES);
       const int k0 = (kb_first + kb) * BK;
-      if (op & OP_A_MN) {        // two 64-row K x 64-column M boxes
+      if (ep.drop_load && kb == 0) {
+        // test hook: the A operand of this stage never arrives
+      } else if (op & OP_A_MN) {        // two 64-row K x 64-column M boxes
         tma_load_2d(&tmA, &full[s], sa, m0, k0);
         tma_load_2d(&tmA, &full[s], sa + 8192, m0 + 64, k0);
       } else {
@@ -199,7 +203,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     if (failed) {
       // Drain: wait (bounded) for the copies still in flight before the block can exit.
       for (int kb = issued > stages ? issued - stages : 0; kb < issued; ++kb)
-        mbar_wait(&full[kb % stages], (uint32_t)(kb / stages) & 1u);
+        mbar_wait(&full[kb % stages], (uint32_t)(kb / stages) & 1u, ep.spin_limit);
     }
   } else if (threadIdx.x == 32) {
     // MMA issuer.
@@ -208,7 +212,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     for (int kb = 0; kb < kblocks && ok; ++kb) {
       const int s = kb % stages;
       const uint32_t round = (uint32_t)(kb / stages);
-      if (!mbar_wait(&full[s], round & 1u)) { atomicExch(&failed, 1); ok = false; break; }
+      if (!mbar_wait(&full[s], round & 1u, ep.spin_limit)) { atomicExch(&failed, 1); ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;");
       const uint32_t a_addr = smem_u32(smem + s * STAGE_BYTES);
       const uint32_t b_addr = a_addr + A_BYTES;
@@ -237,7 +241,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
   // Epilogue: every warp waits for the accumulator, then reads its 32 rows 32 columns at a time
   // (lane = row). Each 32 x 32 block goes through shared memory (the idle stage buffers) so that
   // the global stores are row-contiguous across the warp: lane = column.
-  const bool have = mbar_wait(&done, 0);
+  const bool have = mbar_wait(&done, 0, ep.spin_limit);
   asm volatile("tcgen05.fence::after_thread_sync;");
   __syncwarp();
   const bool good = have && !failed;

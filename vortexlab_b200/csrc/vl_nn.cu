@@ -175,6 +175,8 @@ int vl_nn_gemm_bf16(const void* a, int lda, const void* b, int ldb, int M, int N
   ep.n_valid = N;
   ep.flags = flags & (vl::gemm::EPI_ACCUM | vl::gemm::EPI_BIAS | vl::gemm::EPI_RELU | vl::gemm::EPI_BF16);
   ep.err = err;
+  ep.drop_load = (flags & VL_GEMM_TEST_TIMEOUT) ? 1 : 0;
+  ep.spin_limit = ep.drop_load ? (1u << 12) : vl::gemm::kSpinLimit;
   cudaStream_t s = (cudaStream_t)stream;
   switch (bn) {
     case 32: return launch_gemm<32>(ta, tb, M, N, K, op, ep, s);
