@@ -174,12 +174,15 @@ def run_reference(args):
 
 
 def channel_n80(V):
-    """The reference's own benchmark (`vortexlab bench --n 80 --steps 1000`): MLUPS and state hash."""
+    """The reference's own benchmark (`vortexlab bench --n 80 --steps 1000`): MLUPS and state hash,
+    checked against the hash it publishes (tests/golden/published.json)."""
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", "published.json")) as f:
+        want = set(json.load(f)["bench_state_hashes"]["1762x330"]["hashes"].values())
     ch, secs = V.cylinder.bench(V.cylinder.Setup(n=80), 1000)
     h = ch.sim.state_hash()
     out = {"grid": f"{ch.sim.nx}x{ch.sim.ny}", "fluid_nodes": ch.sim.fluid_nodes(), "steps": 1000,
            "mlups": round(ch.sim.fluid_nodes() * 1000 / secs / 1e6, 1), "ms_per_step": round(secs * 1e3 / 1000, 5),
-           "state_hash": f"{h:016x}", "published_hash_match": f"{h:016x}" == "c93e26bfa33474ee"}
+           "state_hash": f"{h:016x}", "published_hash_match": {f"{h:016x}"} == want}
     ch.close()
     return out
 

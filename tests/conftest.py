@@ -1,3 +1,4 @@
+import json
 import os
 import sys
 
@@ -34,3 +35,11 @@ def gpu(V):
     if V.device_count() == 0:
         pytest.fail("a gpu-marked test ran without a CUDA device")
     return V
+
+
+@pytest.fixture(scope="session")
+def published():
+    """The reference's published known answers (tests/golden/published.json, made by
+    tests/golden/make_published.py from docs/report/index.html:59 and README.md:182-188)."""
+    with open(os.path.join(TESTS, "golden", "published.json")) as f:
+        return json.load(f)

@@ -22,20 +22,16 @@ def _force_close(a, b, rel=FORCE_REL):
     return np.max(np.abs(a - b)) <= rel * scale
 
 
-def test_published_state_hash_n40_3000_steps(gpu):
-    """docs/report/index.html:59: 6b6814b976bbbaff after `vortexlab bench --n 40 --steps 3000`."""
+@pytest.mark.parametrize("grid", ["882x166", "1762x330"])
+def test_published_state_hash(gpu, published, grid):
+    """docs/report/index.html:59: the FNV-1a state hash after `vortexlab bench --n 40 --steps 3000`
+    (882 x 166) and `--n 80 --steps 1000` (1762 x 330), the same for 1, 2 and 4 threads."""
     V = gpu
-    ch, secs = V.cylinder.bench(V.cylinder.Setup(n=40), 3000)
-    assert ch.sim.fluid_nodes() == 143056
-    assert f"{ch.sim.state_hash():016x}" == "6b6814b976bbbaff"
-
-
-def test_published_state_hash_n80_1000_steps(gpu):
-    """docs/report/index.html:59: c93e26bfa33474ee after `vortexlab bench --n 80 --steps 1000`."""
-    V = gpu
-    ch, secs = V.cylinder.bench(V.cylinder.Setup(n=80), 1000)
-    assert ch.sim.fluid_nodes() == 572256
-    assert f"{ch.sim.state_hash():016x}" == "c93e26bfa33474ee"
+    case = published["bench_state_hashes"][grid]
+    ch, secs = V.cylinder.bench(V.cylinder.Setup(n=case["n"]), case["steps"])
+    assert f"{ch.sim.nx}x{ch.sim.ny}" == grid
+    assert ch.sim.fluid_nodes() == case["fluid_nodes"]
+    assert {f"{ch.sim.state_hash():016x}"} == set(case["hashes"].values())
 
 
 def test_config1_channel_n20_1000_steps_against_oracle(gpu, O):
@@ -181,17 +177,13 @@ def test_schedules_and_autotune_do_not_change_results(gpu):
     assert all(x == results[0] for x in results)
 
 
-@pytest.mark.parametrize("n,published", [
-    (20, (3.3244, 3.2719, 0.9807, -1.0175, 0.2988, 2.4700)),
-    (40, (3.2423, 3.1919, 0.9830, -1.0181, 0.3006, 2.4734)),
-    (80, (3.2354, 3.1840, 0.9947, -1.0295, 0.3007, 2.4840)),
-])
-def test_published_2d2_results(gpu, n, published):
+@pytest.mark.parametrize("n", [20, 40, 80])
+def test_published_2d2_results(gpu, published, n):
     """README.md:182-188: the reference's own case-2D-2 results (lattice U 0.05, 100 convective
     units, statistics over the last 20) at 20, 40 and 80 cells per diameter, to the four decimals
     it prints: c_D max / min, c_L max / min, St and the pressure drop."""
     V = gpu
     u = V.cylinder.run_2d2(V.cylinder.Setup(n=n), 100.0, 20.0)
-    got = (u.cd_max, u.cd_min, u.cl_max, u.cl_min, u.st, u.dp)
-    for name, g, p in zip(("cd_max", "cd_min", "cl_max", "cl_min", "st", "dp"), got, published):
+    for name, p in published["case_2d2_u0.05"][str(n)].items():
+        g = getattr(u, name)
         assert abs(g - p) <= 1e-4, (name, g, p)

@@ -13,18 +13,13 @@ import pytest
 import oracle as O
 
 
-def test_oracle_reproduces_published_hash_n40(O):
-    ch, n, xc, yc = O.cylinder_rig(40, threads=8)
-    assert (ch.sim.nx, ch.sim.ny, ch.sim.fluid_nodes()) == (882, 166, 143056)
-    ch.run(3000, record_force=False)
-    assert f"{ch.sim.state_hash():016x}" == "6b6814b976bbbaff"
-
-
-def test_oracle_reproduces_published_hash_n80(O):
-    ch, n, xc, yc = O.cylinder_rig(80, threads=8)
-    assert (ch.sim.nx, ch.sim.ny, ch.sim.fluid_nodes()) == (1762, 330, 572256)
-    ch.run(1000, record_force=False)
-    assert f"{ch.sim.state_hash():016x}" == "c93e26bfa33474ee"
+@pytest.mark.parametrize("grid", ["882x166", "1762x330"])
+def test_oracle_reproduces_published_hash(O, published, grid):
+    case = published["bench_state_hashes"][grid]
+    ch, n, xc, yc = O.cylinder_rig(case["n"], threads=8)
+    assert (f"{ch.sim.nx}x{ch.sim.ny}", ch.sim.fluid_nodes()) == (grid, case["fluid_nodes"])
+    ch.run(case["steps"], record_force=False)
+    assert {f"{ch.sim.state_hash():016x}"} == set(case["hashes"].values())
 
 
 def test_result_does_not_depend_on_thread_count(O):
