@@ -27,10 +27,11 @@ sys.path.insert(0, ROOT)
 BOX = dict(nx=8192, ny=4096, seed=0x5EED0001, fraction=0.05, tau=0.55, u=0.05)
 BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36}
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes per interior-node update of the bulk kernel from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch of the 2048 x 2048 box divided by its interior nodes; see
-# profiles/k_bulk_k_links_f64_disk_box.md), per precision. Scaled to a full launch by nodes.
-NCU_DRAM_BYTES_PER_LU = {"f64": 139.3}
+# DRAM bytes per node update of the bulk kernel from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum of one launch of the 2048 x 2048 box divided by the nodes it updates:
+# interior nodes for the two-kernel step, all fluid nodes for the staged step; see
+# profiles/k_bulk_k_links_f64_disk_box.md), per (precision, staged). Scaled to a full launch by nodes.
+NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3}
 
 
 def workload_name(prec):
@@ -257,16 +258,20 @@ def run_vortexlab(args):
     secs = total_ms_max * 1e-3
     value = world * fluid * args.steps / secs / 1e6
 
-    # roofline of the dominant kernel (the bulk kernel: interior nodes, pull + collide)
+    # roofline of the dominant kernel, the bulk kernel: pull + collide of the interior nodes, or of
+    # every fluid node in the staged step (whose first kernel only evaluates the link rules)
     peak, peak_kind = hbm_peak()
     bpl = BYTES_PER_LU[prec]
+    staged = sim.schedule == "staged"
+    bulk_nodes = fluid if staged else interior
     bulk_launch_s = bulk_ms * 1e-3 / args.steps
-    achieved = interior * bpl / bulk_launch_s / 1e9
-    traffic = NCU_DRAM_BYTES_PER_LU.get(prec)
+    achieved = bulk_nodes * bpl / bulk_launch_s / 1e9
+    traffic = NCU_DRAM_BYTES_PER_LU.get((prec, staged))
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "traffic": None if traffic is None else round(traffic * interior),
-                "kernel": "k_bulk", "algorithmic_bytes_per_launch": interior * bpl,
+                "traffic": None if traffic is None else round(traffic * bulk_nodes),
+                "kernel": "k_bulk (staged: all fluid nodes)" if staged else "k_bulk (interior nodes)",
+                "algorithmic_bytes_per_launch": bulk_nodes * bpl,
                 "kernel_ms_per_launch": round(bulk_ms / args.steps, 4),
                 "link_kernel_ms_per_launch": round(link_ms / args.steps, 4),
                 "bulk_share": round(bulk_ms / max(bulk_ms + link_ms, 1e-12), 4),
@@ -344,7 +349,7 @@ def main():
     ap.add_argument("--precision", choices=["f64", "f32", "f16s"], default="f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
-    ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first"])
+    ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first", "staged"])
     ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
     args = ap.parse_args()
     if args.box:

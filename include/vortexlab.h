@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define VL_ABI_VERSION 1
+#define VL_ABI_VERSION 2
 
 /* ---- status codes */
 #define VL_OK 0
@@ -193,16 +193,22 @@ int vl_sim_last_step_ms(vl_sim* s, float* ms);
  * stream; returns the summed device milliseconds of the link kernels, of the bulk kernels and of
  * the whole batch (any pointer may be NULL). Used to measure each kernel's share of a step. */
 int vl_sim_step_profiled(vl_sim* s, uint64_t steps, double* link_ms, double* bulk_ms, double* total_ms);
-/* Order of the two kernels of each step: VL_SCHEDULE_CONCURRENT (link kernel on a second stream,
- * forked from and joined to the sim's stream), VL_SCHEDULE_LINKS_FIRST or VL_SCHEDULE_BULK_FIRST
- * (one stream). All three give bit-identical results; only the speed differs. */
-enum { VL_SCHEDULE_CONCURRENT = 0, VL_SCHEDULE_LINKS_FIRST = 1, VL_SCHEDULE_BULK_FIRST = 2 };
+/* How each step is launched. VL_SCHEDULE_CONCURRENT: the link kernel (boundary nodes) on a second
+ * stream, forked from and joined to the sim's stream, beside the bulk kernel (interior nodes);
+ * VL_SCHEDULE_LINKS_FIRST / VL_SCHEDULE_BULK_FIRST: the same two kernels in order on one stream;
+ * VL_SCHEDULE_STAGED: a kernel that applies the link rules only (the population each link returns
+ * into the fluid), then a bulk kernel that updates every fluid cell, boundary cells included, in
+ * coalesced row tiles. All four give bit-identical results; only the speed differs. The batch
+ * engine (vl_batch_set_schedule) takes the first three. */
+enum { VL_SCHEDULE_CONCURRENT = 0, VL_SCHEDULE_LINKS_FIRST = 1, VL_SCHEDULE_BULK_FIRST = 2, VL_SCHEDULE_STAGED = 3,
+       VL_SCHEDULE_COUNT = 4 };
 int vl_sim_set_schedule(vl_sim* s, int schedule);
 int vl_sim_get_schedule(const vl_sim* s);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the
- * fastest. ms3 (may be NULL) receives the milliseconds per step of the three schedules. */
-int vl_sim_autotune(vl_sim* s, int steps_each, double* ms3);
+ * fastest. ms (may be NULL) receives the milliseconds per step of the VL_SCHEDULE_COUNT
+ * schedules, in VL_SCHEDULE_* order. */
+int vl_sim_autotune(vl_sim* s, int steps_each, double* ms);
 /* Number of kernel launches issued by this sim so far (steps launch one or two kernels each). */
 int vl_sim_launch_count(vl_sim* s, uint64_t* out);
 

@@ -27,8 +27,9 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
         ch.step(c.steps)
         single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.populations().copy()))
         ch.close()
-    first = None
-    for tile, sched in [("256x1", "concurrent"), ("64x4", "links-first"), ("32x8", "bulk-first")]:
+    first = {}
+    for tile, sched in [("256x1", "concurrent"), ("64x4", "links-first"), ("32x8", "bulk-first"),
+                        ("128x2", "staged"), ("32x8", "staged")]:
         b = Batch(prec)
         for c in cases:
             b.add(c.tunnel.spec(c.body), c.steps)
@@ -45,11 +46,18 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
                 assert hashes[-1] == single[k][0], (tile, sched, k)
                 assert np.array_equal(b.force_history(k), single[k][1]), (tile, sched, k)
             else:
-                assert np.max(np.abs(b.populations(k) - single[k][2])) <= 1e-6, (tile, sched, k)
+                # FP32 rounding: 1e-6 for the kernels shared with the single-tunnel step; the staged
+                # pair collides boundary cells in the bulk kernel, whose multiply-add contraction
+                # rounds differently, and the flow amplifies those last-bit differences to ~2e-6
+                tol, ftol = (1e-5, 1e-3) if sched == "staged" else (1e-6, 1e-4)
+                assert np.max(np.abs(b.populations(k) - single[k][2])) <= tol, (tile, sched, k)
                 h = b.force_history(k)
-                assert np.max(np.abs(h - single[k][1])) <= 1e-4 * np.max(np.abs(single[k][1])), (tile, sched, k)
-        first = first or hashes
-        assert hashes == first, (tile, sched)      # every tile shape and schedule: bit-identical
+                assert np.max(np.abs(h - single[k][1])) <= ftol * np.max(np.abs(single[k][1])), (tile, sched, k)
+        # every tile shape and schedule: bit-identical (FP32 / FP16: the staged pair collides the
+        # boundary cells in the bulk kernel, whose multiply-add contraction may differ in the last bit)
+        group = "all" if prec == "f64" else sched == "staged"
+        first.setdefault(group, hashes)
+        assert hashes == first[group], (tile, sched)
         b.close()
 
 
@@ -58,12 +66,14 @@ def test_batch_autotune_and_partial_runs_do_not_change_results(gpu):
     from vortexlab_b200.batch import Batch
     cases = _cases(V)
     out = []
-    for mode in ("plain", "tuned"):
+    for mode in ("plain", "tuned", "staged plain", "staged tuned"):
         b = Batch("f32")
         for c in cases:
             b.add(c.tunnel.spec(c.body), c.steps)
         b.build()
-        if mode == "tuned":
+        if mode.startswith("staged"):
+            b.schedule = "staged"
+        if mode.endswith("tuned"):
             ms = b.autotune(2)
             assert set(ms) == {"256x1", "128x2", "64x4", "32x8"}
             b.run(37)      # stop in the middle of a segment, then continue
@@ -73,7 +83,7 @@ def test_batch_autotune_and_partial_runs_do_not_change_results(gpu):
         out.append([b.state_hash(k) for k in range(len(cases))])
         assert b.launch_count() >= 2 * max(c.steps for c in cases)
         b.close()
-    assert out[0] == out[1]
+    assert out[0] == out[1] and out[2] == out[3]
 
 
 @pytest.mark.parametrize("prec", ["f64", "f32"])

@@ -156,11 +156,11 @@ def test_graph_and_single_steps_agree(gpu):
 
 
 def test_schedules_and_autotune_do_not_change_results(gpu):
-    """The three kernel orders give bit-identical states; autotuning (dry-run timing) leaves t,
-    the force, the history and the state untouched."""
+    """The four step schedules give bit-identical states and force histories; autotuning (dry-run
+    timing) leaves t, the force, the history and the state untouched."""
     V = gpu
     results = []
-    for sched in ("concurrent", "links-first", "bulk-first", "auto"):
+    for sched in ("concurrent", "links-first", "bulk-first", "staged", "auto"):
         r = V.cylinder.rig(V.cylinder.Setup(n=10), 100.0, 1.0)
         sim = r.ch.sim
         sim.record(300)
@@ -168,7 +168,7 @@ def test_schedules_and_autotune_do_not_change_results(gpu):
         if sched == "auto":
             t0, f0 = sim.t, sim.force.copy()
             ms = sim.autotune(4)
-            assert set(ms) == {"concurrent", "links-first", "bulk-first"}
+            assert set(ms) == {"concurrent", "links-first", "bulk-first", "staged"}
             assert sim.t == t0 and np.array_equal(sim.force, f0)
         else:
             sim.schedule = sched
@@ -187,3 +187,101 @@ def test_published_2d2_results(gpu, published, n):
     for name, p in published["case_2d2_u0.05"][str(n)].items():
         g = getattr(u, name)
         assert abs(g - p) <= 1e-4, (name, g, p)
+
+
+def _staged_cases():
+    from vortexlab_b200.workloads import disk_field
+    return {
+        # 600 is not a multiple of the 256-cell row tile: the last tile of each row is partial
+        "disk_box_600x256": S.disk_box(600, 256, disk_field(600, 256, seed=11)),
+        "tunnel_radiating": S.tunnel_like(radiating=True),
+        "tunnel_walls": S.tunnel_like(radiating=False),
+        "poiseuille_trt": S.poiseuille(rows=16, q=0.8, collision=("trt", 0.25)),
+    }
+
+
+@pytest.mark.parametrize("name", list(_staged_cases()))
+def test_staged_schedule_against_oracle(gpu, O, name):
+    """The staged step (link values first, then row tiles that update boundary cells too) against
+    the oracle on domains with every link rule, forcing and partial row tiles: bit-identical
+    populations, forces within the stated bar."""
+    d = _staged_cases()[name]
+    sim = S.product_sim(d)
+    sim.schedule = "staged"
+    osim = S.oracle_sim(d, threads=4)
+    ny, nx = d["ny"], d["nx"]
+    if "accel" not in d:
+        sim.init((1.0, 0.05, 0.0))
+        osim.init((np.ones((ny, nx)), np.full((ny, nx), 0.05), np.zeros((ny, nx))))
+    for k in range(6):
+        if name.startswith("tunnel"):
+            v1 = 0.5 + 0.05 * k
+            for s in (sim, osim):
+                s.vscale[1] = v1
+                s.vscale[2] = 0.002 * np.sin(0.3 * k)
+                s.outflow_target = 0.05 * v1
+        sim.step(50)
+        osim.step(50)
+        assert _force_close(sim.force, osim.force)
+        assert sim.outlet_density_offset == osim.outlet_density_offset
+    assert np.array_equal(sim.populations(), osim.populations())
+
+
+def test_staged_schedule_reproduces_published_hash(gpu, published):
+    """docs/report/index.html:59 through the staged step: 882 x 166 after 3000 steps."""
+    V = gpu
+    case = published["bench_state_hashes"]["882x166"]
+    r = V.cylinder.rig(V.cylinder.Setup(n=case["n"]), 100.0, 8.0)
+    r.ch.sim.schedule = "staged"
+    r.ch.step(case["steps"])
+    assert {f"{r.ch.sim.state_hash():016x}"} == set(case["hashes"].values())
+
+
+@pytest.mark.parametrize("precision", ["f32", "f16s"])
+def test_staged_schedule_reduced_precision(gpu, precision):
+    """FP32 and FP16-shifted storage through the staged step agree with the two-kernel step to
+    the rounding of their arithmetic (the two pairings may contract multiply-adds differently)."""
+    from vortexlab_b200.workloads import disk_field
+    d = S.disk_box(512, 256, disk_field(512, 256, seed=5))
+    out = []
+    for sched in ("concurrent", "staged"):
+        sim = S.product_sim(d, precision=precision)
+        sim.schedule = sched
+        sim.init((1.0, 0.05, 0.0))
+        sim.step(200)
+        out.append((sim.populations(), sim.force.copy()))
+    tol = 1e-5 if precision == "f32" else 2e-3
+    assert np.max(np.abs(out[0][0] - out[1][0])) <= tol
+    assert np.max(np.abs(out[0][1] - out[1][1])) <= tol * max(1.0, np.max(np.abs(out[0][1])))
+
+
+def test_staged_schedule_follows_every_change_of_state(gpu):
+    """The staged step keeps a compact copy of the boundary nodes' populations. It must follow the
+    state through schedule switches, uploads, re-initialisation and autotuning: the same sequence
+    of operations through the two-kernel step gives the same bits."""
+    from vortexlab_b200.workloads import disk_field
+    d = S.disk_box(320, 160, disk_field(320, 160, seed=9))
+    donor = S.product_sim(d)
+    donor.init((1.0, 0.04, 0.01))
+    donor.step(70)
+    f_up = donor.populations()
+    out = []
+    for staged in (False, True):
+        sim = S.product_sim(d)
+        first = "staged" if staged else "concurrent"
+        sim.schedule = first
+        sim.init((1.0, 0.05, 0.0))
+        sim.step(33)                      # graph of 32 steps + one launch
+        sim.schedule = "links-first"
+        sim.step(5)
+        sim.schedule = first
+        sim.step(7)
+        sim.set_populations(f_up)         # the state set from the host
+        sim.step(40)
+        sim.autotune(2)                   # dry timing of every schedule, then the fastest
+        sim.schedule = first
+        sim.step(9)
+        sim.init((1.0, 0.02, -0.01))      # re-initialised
+        sim.step(12)
+        out.append((sim.state_hash(), sim.force.tobytes()))
+    assert out[0] == out[1]

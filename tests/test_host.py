@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol(V):
     missing = [s for s in sorted(declared_symbols()) if not hasattr(lib, s)]
     assert not missing, missing
     assert set(_lib.DECLARED) <= declared_symbols()
-    assert V.lib.vl_abi_version() == 1
+    assert V.lib.vl_abi_version() == 2
 
 
 def test_no_cpu_fallback_without_a_device(V):
@@ -170,3 +170,41 @@ def test_disk_field_is_seeded_and_reaches_the_fraction():
     frac = solid.mean()
     assert 0.05 <= frac < 0.052
     assert np.all(a[:, 2] >= 4.0) and np.all(a[:, 2] <= 16.0)
+
+
+@pytest.mark.parametrize("name", list(_domains().keys()))
+def test_staged_step_lookup(V, name):
+    """The staged bulk kernel finds a boundary cell's node and links from the row tile alone: the
+    node's CSR rank is the warp slot's first rank plus the boundary cells before the lane, and the
+    link of direction j is first + popc(mask below j). Replayed here on the host tables, for every
+    boundary cell, with the kernel's tiling (256-cell row tiles, 32-cell warp slots)."""
+    t = S.product_builder(_domains()[name]).link_table()
+    flags, bidx, bfirst, dirs = t["flags"], t["bnode_idx"], t["bnode_first"], t["link_i32"][:, 0]
+    ny, nx = flags.shape
+    nb = len(bidx)
+    mask = np.zeros(nb, dtype=np.int64)
+    for k in range(nb):
+        d = dirs[bfirst[k]:bfirst[k + 1]]
+        assert np.all(np.diff(d) > 0) and d.min() >= 1 and d.max() <= 8
+        mask[k] = np.bitwise_or.reduce(1 << d.astype(np.int64))
+    flat = flags.reshape(-1)
+    before = np.concatenate([[0], np.cumsum(flat == 1)])  # boundary cells before each cell
+    tiles = (nx + 255) // 256
+    seen = 0
+    for y in range(ny):
+        for w in range(tiles * 8):
+            x0 = w * 32
+            lanes = np.arange(x0, min(x0 + 32, nx))
+            if len(lanes) == 0:
+                continue
+            first = before[y * nx + x0]
+            row = flat[y * nx + lanes]
+            for r, x in enumerate(lanes[row == 1]):
+                k = first + r
+                assert k < nb and bidx[k] == y * nx + x
+                for j in range(1, 9):
+                    if mask[k] >> j & 1:
+                        l = bfirst[k] + bin(int(mask[k]) & ((1 << j) - 1)).count("1")
+                        assert bfirst[k] <= l < bfirst[k + 1] and dirs[l] == j
+                seen += 1
+    assert seen == nb

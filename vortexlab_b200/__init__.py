@@ -632,7 +632,7 @@ class Sim:
         check(lib.vl_sim_step_profiled(self._h, n, C.byref(lk), C.byref(bk), C.byref(tot)))
         return lk.value, bk.value, tot.value
 
-    SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2}
+    SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2, "staged": 3}
 
     @property
     def schedule(self) -> str:
@@ -644,9 +644,9 @@ class Sim:
         check(lib.vl_sim_set_schedule(self._h, self.SCHEDULES[name]))
 
     def autotune(self, steps_each: int = 8):
-        """Times the three kernel schedules without advancing the state; keeps the fastest.
+        """Times the four kernel schedules without advancing the state; keeps the fastest.
         Returns {schedule: ms per step}."""
-        out = np.zeros(3)
+        out = np.zeros(len(self.SCHEDULES))
         check(lib.vl_sim_autotune(self._h, steps_each, _dp(out)))
         return dict(zip(self.SCHEDULES, out.tolist()))
 

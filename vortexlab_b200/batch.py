@@ -27,7 +27,7 @@ def _dp(a):
 
 
 class Batch:
-    SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2}
+    SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2, "staged": 3}
     TILES = {(8, 1): "256x1", (7, 2): "128x2", (6, 4): "64x4", (5, 8): "32x8"}
 
     def __init__(self, precision="f32"):

@@ -206,7 +206,7 @@ def warm_comparison(net, cases, refs=None, precision="f32", tol=0.005):
     return dict(summary=summary, rows=rows)
 
 
-def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0):
+def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0, schedule="concurrent"):
     """The full seeded batch: MLUPS of the whole run (or of its first `max_steps` global steps)."""
     from .batch import Batch, seeded_tunnels
     cases = seeded_tunnels(seed=seed, count=count, precision=precision)
@@ -216,6 +216,7 @@ def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0):
         b.add(c.tunnel.spec(c.body), c.steps)
     b.build()
     setup = time.perf_counter() - t0
+    b.schedule = schedule
     tune = b.autotune(3)
     b.run(max_steps)
     ms = b.last_run_ms()
@@ -224,7 +225,8 @@ def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0):
         t, nonfinite, _ = b.status(k)
         lu += b.info(k)["fluid_nodes"] * t
     out = dict(tunnels=count, precision=precision, global_steps=b.global_step(), lattice_updates=lu,
-               seconds=ms * 1e-3, mlups=lu / (ms * 1e-3) / 1e6, tile=b.tile, autotune_ms_per_step=tune,
+               seconds=ms * 1e-3, mlups=lu / (ms * 1e-3) / 1e6, tile=b.tile, schedule=schedule,
+               autotune_ms_per_step=tune,
                setup_s=setup, launches=b.launch_count(),
                diverged=[k for k in range(count) if b.status(k)[1]])
     b.close()
@@ -236,6 +238,7 @@ if __name__ == "__main__":
     import sys
     what = sys.argv[1] if len(sys.argv) > 1 else "study"
     if what == "throughput":
-        print(json.dumps(throughput(max_steps=int(sys.argv[2]) if len(sys.argv) > 2 else 0), default=float))
+        print(json.dumps(throughput(max_steps=int(sys.argv[2]) if len(sys.argv) > 2 else 0,
+                                    schedule=sys.argv[3] if len(sys.argv) > 3 else "concurrent"), default=float))
     else:
         print(json.dumps(study(subset=int(sys.argv[2]) if len(sys.argv) > 2 else 32), default=float, indent=1))

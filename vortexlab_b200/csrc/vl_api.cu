@@ -77,6 +77,12 @@ struct vl_sim {
   double* d_red = nullptr;
   int32_t* d_cells = nullptr;
   double* d_gather = nullptr;
+  int2* d_bdesc = nullptr;         // staged step: per boundary node {first link, link-direction mask}
+  int32_t* d_wbfirst = nullptr;    // staged step: boundary nodes before each 32-cell warp slot
+  void* d_lb = nullptr;            // staged step: returning population per link
+  void* d_ownc = nullptr;          // staged step: boundary nodes' own populations (CSR order)
+  bool own_ok = false;             // d_ownc holds the boundary nodes of the current state
+  int split_links = 0, split_tiles = 0;  // staged step in two parts (0: one part)
   cudaStream_t stream = nullptr;   // the sim's stream: bulk kernel, copies, everything else
   cudaStream_t aux = nullptr;      // the link kernel of each step, forked from and joined to `stream`
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -85,9 +91,11 @@ struct vl_sim {
   int ck = 1;
   cudaGraphExec_t gexec = nullptr;
   uint64_t launches = 0;
-  int kernels_per_step = 1;
-  // Order of the two kernels of a step: 0 concurrent (fork/join over two streams), 1 link kernel
-  // then bulk kernel on one stream, 2 bulk then link.
+  int kernels_per_step = 1;  // kernel launches of one step (twice that for the staged step in two parts)
+  uint64_t step_launches() const { return (uint64_t)kernels_per_step * (schedule == 3 && split_links > 0 ? 2 : 1); }
+  // How a step is launched: 0 concurrent (fork/join over two streams), 1 link kernel then bulk
+  // kernel on one stream, 2 bulk then link, 3 staged (link values, then the bulk kernel that also
+  // updates boundary cells; one stream).
   int schedule = 0;
   uint64_t t_host = 0;
   uint64_t rec_start = 0, rec_cap = 0;
@@ -99,7 +107,7 @@ struct vl_sim {
     if (device >= 0) cudaSetDevice(device);
     if (gexec) cudaGraphExecDestroy(gexec);
     void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_ctl,
-                    d_partials, d_hist, d_sched, d_red, d_cells, d_gather};
+                    d_partials, d_hist, d_sched, d_red, d_cells, d_gather, d_bdesc, d_wbfirst, d_lb, d_ownc};
     for (void* p : ptrs)
       if (p) cudaFree(p);
     for (cudaEvent_t e : pev) cudaEventDestroy(e);
@@ -132,21 +140,23 @@ struct vl_sim {
                            cudaEvent_t bk1 = nullptr) {
     cudaError_t e;
     cudaStream_t ls = schedule == 0 ? aux : stream;
+    const int staged = schedule == 3 ? 0x400 : 0;
     auto links = [&]() -> cudaError_t {
       cudaError_t r;
       if (lk0 && (r = cudaEventRecord(lk0, ls)) != cudaSuccess) return r;
-      if ((r = L->step(P, ck | 0x100, a(), b(), ls)) != cudaSuccess) return r;
+      if ((r = L->step(P, ck | 0x100 | staged, a(), b(), ls)) != cudaSuccess) return r;
       if (lk1 && (r = cudaEventRecord(lk1, ls)) != cudaSuccess) return r;
       return cudaSuccess;
     };
     auto bulk = [&]() -> cudaError_t {
       cudaError_t r;
       if (bk0 && (r = cudaEventRecord(bk0, stream)) != cudaSuccess) return r;
-      if ((r = L->step(P, ck | 0x200, a(), b(), stream)) != cudaSuccess) return r;
+      if ((r = L->step(P, ck | 0x200 | staged, a(), b(), stream)) != cudaSuccess) return r;
       if (bk1 && (r = cudaEventRecord(bk1, stream)) != cudaSuccess) return r;
       return cudaSuccess;
     };
-    if (schedule == 1) {
+    if (schedule == 3 && split_links > 0) return enqueue_staged_split(lk0, lk1, bk0, bk1);
+    if (schedule == 1 || schedule == 3) {
       if ((e = links()) != cudaSuccess) return e;
       return bulk();
     }
@@ -162,8 +172,39 @@ struct vl_sim {
     return cudaStreamWaitEvent(stream, ev_join, 0);
   }
 
+  // The staged step in two parts. The first `split_links` link blocks run first; then the bulk
+  // tiles of the rows whose boundary nodes they hold (`split_tiles` tiles), while the remaining link
+  // blocks run beside them on `aux`; then the remaining tiles, after both. Only the first part of
+  // the link kernel is exposed. The events bracket the exposed link part and the two bulk parts.
+  cudaError_t enqueue_staged_split(cudaEvent_t lk0, cudaEvent_t lk1, cudaEvent_t bk0, cudaEvent_t bk1) {
+    cudaError_t e;
+    vl::StepParams pa = P, pb = P;
+    pa.link_b0 = 0;
+    pa.link_n = split_links;
+    pa.bulk_b0 = 0;
+    pa.bulk_n = split_tiles;
+    pb.link_b0 = split_links;
+    pb.link_n = P.nlink - split_links;
+    pb.bulk_b0 = split_tiles;
+    pb.bulk_n = P.nbulk - split_tiles;
+    const int lk = ck | 0x100 | 0x400, bk = ck | 0x200 | 0x400;
+    if ((e = cudaEventRecord(ev_fork, stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(aux, ev_fork, 0)) != cudaSuccess) return e;
+    if (lk0 && (e = cudaEventRecord(lk0, stream)) != cudaSuccess) return e;
+    if ((e = L->step(pa, lk, a(), b(), stream)) != cudaSuccess) return e;
+    if (lk1 && (e = cudaEventRecord(lk1, stream)) != cudaSuccess) return e;
+    if ((e = L->step(pb, lk, a(), b(), aux)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(ev_join, aux)) != cudaSuccess) return e;
+    if (bk0 && (e = cudaEventRecord(bk0, stream)) != cudaSuccess) return e;
+    if ((e = L->step(pa, bk, a(), b(), stream)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(stream, ev_join, 0)) != cudaSuccess) return e;
+    if ((e = L->step(pb, bk, a(), b(), stream)) != cudaSuccess) return e;
+    if (bk1 && (e = cudaEventRecord(bk1, stream)) != cudaSuccess) return e;
+    return cudaSuccess;
+  }
+
   int set_schedule(int sc) {
-    if (sc < 0 || sc > 2) return fail(VL_EINVAL, "schedule must be 0, 1 or 2");
+    if (sc < 0 || sc >= VL_SCHEDULE_COUNT) return fail(VL_EINVAL, "schedule must be 0, 1, 2 or 3");
     if (sc != schedule && gexec) {
       VL_CUDA(cudaStreamSynchronize(stream));
       cudaGraphExecDestroy(gexec);
@@ -183,8 +224,10 @@ struct vl_sim {
     if ((rc = push_ctl())) return rc;
     double best = 1e300;
     int best_sc = schedule;
-    for (int sc = 0; sc < 3; ++sc) {
+    for (int sc = 0; sc < VL_SCHEDULE_COUNT; ++sc) {
       schedule = sc;
+      own_ok = false;
+      if ((rc = prepare_steps())) return rc;
       for (int k = 0; k < 2; ++k) {
         cudaError_t e = enqueue_step();
         if (e != cudaSuccess) return cuda_fail(e, "autotune");
@@ -201,6 +244,8 @@ struct vl_sim {
       if (ms_out) ms_out[sc] = ms / steps_each;
       if (ms < best) { best = ms; best_sc = sc; }
     }
+    // the dry staged steps left the copy of `b`, not of `a`
+    own_ok = false;
     if ((rc = pull_ctl())) return rc;
     hctl.dry = 0;
     if ((rc = push_ctl())) return rc;
@@ -218,11 +263,22 @@ struct vl_sim {
     return VL_OK;
   }
 
+  // The staged step reads the boundary nodes' own populations from d_ownc, which each staged bulk
+  // kernel refreshes for the next step; after anything else set the state it is gathered from `a`.
+  int prepare_steps() {
+    if (schedule != 3 || own_ok) return VL_OK;
+    cudaError_t e = L->gather_own(P, a(), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "gather own populations");
+    launches += 1;
+    own_ok = true;
+    return VL_OK;
+  }
+
   int launch_one() {
     cudaError_t e = enqueue_step();
     if (e != cudaSuccess) return cuda_fail(e, "step launch");
     cur ^= 1;
-    launches += (uint64_t)kernels_per_step;
+    launches += step_launches();
     return VL_OK;
   }
 
@@ -252,6 +308,7 @@ struct vl_sim {
 
   int step(uint64_t steps) {
     VL_CUDA(cudaSetDevice(device));
+    if (int rc = prepare_steps()) return rc;
     VL_CUDA(cudaEventRecord(ev0, stream));
     uint64_t left = steps;
     while (left > 0) {
@@ -259,7 +316,7 @@ struct vl_sim {
         int rc = ensure_graph();
         if (rc) return rc;
         VL_CUDA(cudaGraphLaunch(gexec, stream));
-        launches += (uint64_t)kGraphSteps * kernels_per_step;
+        launches += (uint64_t)kGraphSteps * step_launches();
         left -= kGraphSteps;
       } else {
         int rc = launch_one();
@@ -270,6 +327,7 @@ struct vl_sim {
     VL_CUDA(cudaEventRecord(ev1, stream));
     timed = true;
     t_host += steps;
+    if (steps) own_ok = schedule == 3;
     return flush_probe();
   }
 
@@ -284,14 +342,16 @@ struct vl_sim {
       VL_CUDA(cudaEventCreate(&e));
       pev.push_back(e);
     }
+    if (int rc = prepare_steps()) return rc;
     VL_CUDA(cudaEventRecord(pev[0], stream));
     for (uint64_t k = 0; k < steps; ++k) {
       cudaEvent_t* e4 = &pev[2 + 4 * k];
       cudaError_t e = enqueue_step(e4[0], e4[1], e4[2], e4[3]);
       if (e != cudaSuccess) return cuda_fail(e, "profiled step");
       cur ^= 1;
-      launches += (uint64_t)kernels_per_step;
+      launches += step_launches();
     }
+    own_ok = schedule == 3;
     VL_CUDA(cudaEventRecord(pev[1], stream));
     VL_CUDA(cudaEventSynchronize(pev[1]));
     double lk = 0.0, bk = 0.0;
@@ -379,6 +439,41 @@ int alloc_copy(void** dst, const void* src, size_t bytes) {
   VL_CUDA(cudaMalloc(dst, bytes));
   if (src) VL_CUDA(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
   return VL_OK;
+}
+
+// Tables of the staged step. bdesc[k] = {first link of boundary node k, bit j set for each of its
+// link directions j}; the node's links must be stored by ascending direction, so that the link of
+// direction j is first + popc(mask below j). wbfirst[w] = boundary nodes (CSR order = cell order)
+// before the first cell of warp slot w of the bulk grid (block = row tile, 32 cells per warp).
+bool staged_tables(const vl::CompiledDomain& d, int tiles_per_row, std::vector<int2>& bdesc,
+                   std::vector<int32_t>& wbfirst, std::string& err) {
+  const size_t nb = d.bnode_idx.size();
+  bdesc.assign(nb ? nb : 1, int2{0, 0});
+  for (size_t k = 0; k < nb; ++k) {
+    const int first = d.bnode_first[k], last = d.bnode_first[k + 1];
+    int mask = 0, prev = 0;
+    for (int l = first; l < last; ++l) {
+      const int j = d.links[(size_t)l].dir;
+      if (j <= prev || j > 8) { err = "staged step: links of a node must have ascending directions 1..8"; return false; }
+      prev = j;
+      mask |= 1 << j;
+    }
+    bdesc[k] = int2{first, mask};
+  }
+  const int wpt = vl::kBlock / 32;
+  wbfirst.assign((size_t)tiles_per_row * d.ny * wpt, 0);
+  size_t k = 0;  // boundary nodes before the current cell
+  for (size_t y = 0; y < d.ny; ++y) {
+    for (int t = 0; t < tiles_per_row; ++t) {
+      for (int w = 0; w < wpt; ++w) {
+        const size_t x0 = (size_t)t * vl::kBlock + (size_t)w * 32;
+        const size_t start = y * d.nx + std::min(x0, d.nx);
+        while (k < nb && (size_t)d.bnode_idx[k] < start) ++k;
+        wbfirst[(y * tiles_per_row + t) * wpt + w] = (int32_t)k;
+      }
+    }
+  }
+  return true;
 }
 
 // Creates the device-resident sim for a compiled domain.
@@ -478,6 +573,39 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   if (!chk(alloc_copy((void**)&s->d_partials, nullptr, (size_t)P.nlink * 2 * vl::kMaxGroups * sizeof(double))))
     return nullptr;
   P.partials = s->d_partials;
+  // Staged step: node descriptors, per-warp boundary ranks and the per-link output.
+  std::vector<int2> bdesc;
+  std::vector<int32_t> wbfirst;
+  std::string serr;
+  if (!staged_tables(d, P.tiles_per_row, bdesc, wbfirst, serr)) {
+    fail(VL_EINVAL, serr.c_str());
+    return nullptr;
+  }
+  const size_t r_elem = precision == VL_F64 ? sizeof(double) : sizeof(float);
+  if (!chk(alloc_copy((void**)&s->d_bdesc, bdesc.data(), bdesc.size() * sizeof(int2))) ||
+      !chk(alloc_copy((void**)&s->d_wbfirst, wbfirst.data(), wbfirst.size() * sizeof(int32_t))) ||
+      !chk(alloc_copy(&s->d_lb, nullptr, d.links.size() * r_elem)))
+    return nullptr;
+  P.nbs = (unsigned)((nb + 63) / 64 * 64);
+  if (!chk(alloc_copy(&s->d_ownc, nullptr, (size_t)P.nbs * 9 * s->L->elem))) return nullptr;
+  P.link_b0 = 0;
+  P.link_n = P.nlink;
+  P.bulk_b0 = 0;
+  P.bulk_n = P.nbulk;
+  // Split point of the staged step: a quarter of the link blocks, and the row tiles before the row
+  // of the first boundary node they leave to the second part.
+  if (P.nlink >= 4) {
+    const int la = P.nlink / 4;
+    const int row = d.bnode_idx[(size_t)la * vl::kBlock] / (int)d.nx;
+    if (row > 0) {
+      s->split_links = la;
+      s->split_tiles = row * P.tiles_per_row;
+    }
+  }
+  P.bdesc = s->d_bdesc;
+  P.warp_bfirst = s->d_wbfirst;
+  P.lb = s->d_lb;
+  P.ownc = s->d_ownc;
   // Control block: vscale = 1, no outflow target (src/sim.rs:344-347).
   std::memset(&s->hctl, 0, sizeof(vl::Ctl));
   for (int g = 0; g < 4; ++g) s->hctl.vscale[g] = 1.0;
@@ -761,6 +889,7 @@ int vl_sim_init(vl_sim* s, const double* rho, const double* ux, const double* uy
     if (e == cudaSuccess) e = e2;
   }
   if (e != cudaSuccess) return cuda_fail(e, "init");
+  s->own_ok = false;
   // t = 0 (src/sim.rs:370); the force and the outlet offset restart from zero.
   int rc = s->pull_ctl();
   if (rc) return rc;
@@ -868,6 +997,7 @@ int vl_sim_download(vl_sim* s, double* out) {
 int vl_sim_upload(vl_sim* s, const double* in) {
   if (!s || !in) return fail(VL_EINVAL, "null argument");
   VL_CUDA(cudaSetDevice(s->device));
+  s->own_ok = false;
   const size_t n = s->n;
   if (s->prec == VL_F64) {
     VL_CUDA(cudaMemcpy2DAsync(s->buf[s->cur], (size_t)s->ns * 8, in, n * 8, n * 8, 9, cudaMemcpyHostToDevice, s->stream));

@@ -4,7 +4,8 @@
 // Global step s advances every tunnel that still has steps to run. Between the steps at which some
 // tunnel finishes, the set of active tunnels is fixed: that stretch ("segment") uses one tile list
 // and one link-chunk list and is replayed from a captured CUDA graph of 32 steps. Each step is the
-// batched link kernel (on a forked stream) and the batched bulk kernel, as for a single sim.
+// batched link kernel and the batched bulk kernel, scheduled as for a single sim (concurrent on a
+// forked stream, either order on one stream, or the staged pair).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -22,6 +23,8 @@
 namespace {
 
 int fail(int code, const std::string& m) { return vl::set_error(code, m.c_str()); }
+
+bool precision_is_f64(int prec) { return prec == VL_F64; }
 
 int cuda_fail(cudaError_t e, const char* what) {
   return fail(e == cudaErrorMemoryAllocation ? VL_ENOMEM : VL_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -70,6 +73,11 @@ struct vl_batch {
   int4* d_chunks = nullptr;
   double* d_partials = nullptr;
   double* d_hist = nullptr;
+  int2* d_bdesc = nullptr;               // staged step: per boundary node {first link, direction mask}
+  int32_t* d_segb = nullptr;             // staged step: boundary nodes before each 32-cell row segment
+  void* d_lb = nullptr;                  // staged step: returning population per link
+  void* d_ownc = nullptr;                // staged step: boundary nodes' own populations
+  bool own_ok = false;                   // d_ownc holds the active tunnels' current boundary nodes
   cudaStream_t stream = nullptr, aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev0 = nullptr, ev1 = nullptr;
   vl::BatchParams P{};
@@ -86,7 +94,7 @@ struct vl_batch {
     cudaSetDevice(device);
     if (gexec) cudaGraphExecDestroy(gexec);
     void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_sched,
-                    d_tun, d_st, d_tiles, d_chunks, d_partials, d_hist};
+                    d_tun, d_st, d_tiles, d_chunks, d_partials, d_hist, d_bdesc, d_segb, d_lb, d_ownc};
     for (void* p : ptrs)
       if (p) cudaFree(p);
     cudaEvent_t evs[] = {ev_fork, ev_join, ev0, ev1};
@@ -134,8 +142,23 @@ struct vl_batch {
     return VL_OK;
   }
 
+  // The staged step reads the boundary nodes' own populations from d_ownc; after anything other
+  // than a staged step set the state they are gathered from `a` for the active tunnels.
+  int prepare_steps() {
+    if (schedule != 3 || own_ok) return VL_OK;
+    cudaError_t e = L->batch_gather_own(P, nchunks, a(), stream);
+    if (e != cudaSuccess) return cuda_fail(e, "batch gather own populations");
+    launches += 1;
+    own_ok = true;
+    return VL_OK;
+  }
+
   cudaError_t enqueue_step() {
     cudaError_t e;
+    if (schedule == 3) {
+      if ((e = L->batch_step(P, ntiles, nchunks, 1 | 4, a(), b(), stream)) != cudaSuccess) return e;
+      return L->batch_step(P, ntiles, nchunks, 2 | 4, a(), b(), stream);
+    }
     cudaStream_t ls = schedule == 0 ? aux : stream;
     if (schedule == 0) {
       if ((e = cudaEventRecord(ev_fork, stream)) != cudaSuccess) return e;
@@ -187,6 +210,7 @@ struct vl_batch {
         if (T.steps > s) seg_end = std::min<uint64_t>(seg_end, T.steps);
       int rc = build_lists(false);
       if (rc) return rc;
+      if ((rc = prepare_steps())) return rc;
       while (s < seg_end) {
         if (seg_end - s >= (uint64_t)kGraphSteps && (s & 1) == 0) {
           rc = ensure_graph();
@@ -201,6 +225,7 @@ struct vl_batch {
           launches += 2;
         }
       }
+      own_ok = schedule == 3;
     }
     VB_CUDA(cudaEventRecord(ev1, stream));
     VB_CUDA(cudaStreamSynchronize(stream));
@@ -221,6 +246,7 @@ struct vl_batch {
       ty = shapes[c][1];
       int rc = build_lists(false);
       if (rc) { P.dry = 0; return rc; }
+      if ((rc = prepare_steps())) { P.dry = 0; return rc; }
       for (int k = 0; k < steps_each + 2; ++k) {
         if (k == 2) VB_CUDA(cudaEventRecord(ev0, stream));
         cudaError_t e = enqueue_step();
@@ -234,6 +260,7 @@ struct vl_batch {
       if (ms < best) { best = ms; bi = c; }
     }
     P.dry = 0;
+    own_ok = false;  // the dry staged steps left the copy of `b`, not of `a`
     log2_tx = shapes[bi][0];
     ty = shapes[bi][1];
     timed = false;
@@ -290,6 +317,8 @@ int vl_batch_build(vl_batch* b) {
   std::vector<int8_t> pn;
   std::vector<vl::LinkRecDev> links;
   std::vector<double> sched;
+  std::vector<int2> bdesc;
+  std::vector<int32_t> segb;
   unsigned long long pop = 0, cells = 0, hist = 0;
   int nchunk = 0;
   b->tun.resize(nt);
@@ -327,6 +356,29 @@ int vl_batch_build(vl_batch* b) {
     const int32_t loff = (int32_t)links.size();
     for (int32_t v : d.bnode_idx) bidx.push_back(v);
     for (size_t j = 0; j + 1 < d.bnode_first.size(); ++j) bfirst.push_back(d.bnode_first[j] + loff);
+    // Staged-step tables: node descriptors (links by ascending direction) and, per 32-cell row
+    // segment, the global rank of the first boundary node at or after the segment's first cell.
+    for (size_t j = 0; j + 1 < d.bnode_first.size(); ++j) {
+      int mask = 0, prev = 0;
+      for (int l = d.bnode_first[j]; l < d.bnode_first[j + 1]; ++l) {
+        const int dir = d.links[(size_t)l].dir;
+        if (dir <= prev || dir > 8) return fail(VL_EINVAL, "staged step: links of a node must have ascending directions");
+        prev = dir;
+        mask |= 1 << dir;
+      }
+      bdesc.push_back(int2{d.bnode_first[j] + loff, mask});
+    }
+    T.segs = (T.nx + 31) / 32;
+    T.seg_off = (int)segb.size();
+    {
+      size_t kb = 0;
+      for (size_t y = 0; y < d.ny; ++y)
+        for (int sg = 0; sg < T.segs; ++sg) {
+          const size_t start = y * d.nx + (size_t)sg * 32;
+          while (kb < d.bnode_idx.size() && (size_t)d.bnode_idx[kb] < start) ++kb;
+          segb.push_back(T.b_off + (int32_t)kb);
+        }
+    }
     for (const vl::LinkRec& h : d.links) {
       vl::LinkRecDev g;
       g.q = h.q; g.cu6 = h.cu6; g.uw0 = h.uw[0]; g.uw1 = h.uw[1]; g.rho = h.rho;
@@ -345,7 +397,8 @@ int vl_batch_build(vl_batch* b) {
     nchunk += T.nchunks;
   }
   bfirst.push_back((int32_t)links.size());
-  if (links.size() > 0x7fffffffu || cells > 0xFFFFFFFFull) return fail(VL_EINVAL, "batch too large");
+  if (links.size() > 0x7fffffffu || cells > 0xFFFFFFFFull || segb.size() > 0x7fffffffu)
+    return fail(VL_EINVAL, "batch too large");
   const size_t pop_bytes = pop * b->L->elem;
   VB_CUDA(cudaMalloc(&b->buf[0], pop_bytes));
   VB_CUDA(cudaMalloc(&b->buf[1], pop_bytes));
@@ -357,6 +410,11 @@ int vl_batch_build(vl_batch* b) {
   std::vector<vl::BatchState> st(nt);
   std::memset(st.data(), 0, st.size() * sizeof(vl::BatchState));
   if ((rc = upload(&b->d_st, st))) return rc;
+  if ((rc = upload(&b->d_bdesc, bdesc)) || (rc = upload(&b->d_segb, segb))) return rc;
+  const size_t r_elem = precision_is_f64(b->prec) ? sizeof(double) : sizeof(float);
+  const unsigned nbs = (unsigned)((bidx.size() + 63) / 64 * 64);
+  VB_CUDA(cudaMalloc(&b->d_lb, std::max<size_t>(links.size() * r_elem, 16)));
+  VB_CUDA(cudaMalloc(&b->d_ownc, std::max<size_t>((size_t)nbs * 9 * b->L->elem, 16)));
   VB_CUDA(cudaMalloc(&b->d_chunks, std::max<size_t>(b->chunks_all.size(), 1) * sizeof(int4)));
   VB_CUDA(cudaMalloc(&b->d_partials, std::max(nchunk, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaMalloc(&b->d_hist, std::max<unsigned long long>(hist, 1) * 2 * sizeof(double)));
@@ -406,6 +464,11 @@ int vl_batch_build(vl_batch* b) {
   P.hist = b->d_hist;
   P.sqrt_cs2 = std::sqrt(1.0 / 3.0);
   P.dry = 0;
+  P.bdesc = b->d_bdesc;
+  P.seg_bfirst = b->d_segb;
+  P.lb = b->d_lb;
+  P.ownc = b->d_ownc;
+  P.nbs = nbs;
   b->built = true;
   // The host plans (domains) are no longer needed on the host except their sizes.
   for (auto& pl : b->plans) {
@@ -443,7 +506,7 @@ int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty) {
 }
 
 int vl_batch_set_schedule(vl_batch* b, int schedule) {
-  if (!b || schedule < 0 || schedule > 2) return fail(VL_EINVAL, "schedule must be 0, 1 or 2");
+  if (!b || schedule < 0 || schedule >= VL_SCHEDULE_COUNT) return fail(VL_EINVAL, "schedule must be 0, 1, 2 or 3");
   b->schedule = schedule;
   if (b->gexec) {
     cudaGraphExecDestroy(b->gexec);
@@ -567,6 +630,7 @@ int vl_batch_init(vl_batch* b, int k, const double* rho, const double* ux, const
   if (!b || !b->built || !rho || !ux || !uy || k < 0 || (size_t)k >= b->tun.size())
     return fail(VL_EINVAL, "bad arguments");
   if (b->s != 0) return fail(VL_EINVAL, "a tunnel can only be initialised before the batch's first step");
+  b->own_ok = false;
   const size_t n = b->plans[k].dom.n;
   const vl::BatchTunnel& T = b->tun[k];
   double* field = nullptr;
@@ -589,6 +653,7 @@ int vl_batch_init_grid(vl_batch* b, int k, const float* grid, int gh, int gw, in
       !(dy > 0.0))
     return fail(VL_EINVAL, "bad arguments");
   if (b->s != 0) return fail(VL_EINVAL, "a tunnel can only be initialised before the batch's first step");
+  b->own_ok = false;
   const vl::BatchTunnel& T = b->tun[k];
   const size_t n = b->plans[k].dom.n;
   cudaError_t e = b->L->init_grid(T.nx, (int)n, T.ns, b->d_flag + T.cell_off, grid, gh, gw, gc, x0, dx, y0, dy, u,

@@ -12,6 +12,12 @@
 // in a batch is bit-identical to the same tunnel run alone; the FP32 / FP16 kernels are compiled
 // with contraction, which may fuse differently here and in the single-sim kernels (last-bit
 // differences).
+//
+// The staged pairing works as for a single sim: k_batch_links<S, 1> evaluates the link rules of
+// every chunk into the per-link array, then k_batch_bulk<S, 1> updates every fluid cell of its
+// tiles, boundary cells included, and refreshes the compact copy of the boundary nodes' own
+// populations. A warp of a tile (tiles are at least 32 cells wide) covers one 32-cell row segment,
+// whose first boundary-node rank comes from the per-tunnel segment table.
 #pragma once
 
 #include "vl_device.cuh"
@@ -27,6 +33,7 @@ struct BatchTunnel {
   int b_off, nb;                // boundary nodes (global index of the first, count)
   int p_off, np;                // outlet nodes
   int chunk_off, nchunks;       // link chunks
+  int seg_off, segs;            // staged step: first entry and row length (ceil(nx / 32)) in the segment table
   double op, om;
   double u_ref;
   int absorbing;
@@ -62,6 +69,15 @@ struct BatchParams {
   double* hist;                 // 2 doubles per recorded step
   double sqrt_cs2;
   int dry;                      // timing runs: commit nothing
+  // Staged step only (global boundary-node and link indices): per node {first link, link-direction
+  // mask}; per 32-cell row segment of each tunnel, the boundary nodes before it; the population each
+  // link returns into the fluid (arithmetic type); the nodes' own populations (stored type, 9 planes
+  // of stride nbs).
+  const int2* bdesc;
+  const int32_t* seg_bfirst;
+  void* lb;
+  void* ownc;
+  unsigned nbs;
 };
 
 // Controls of a tunnel at its step t (src/cases/channel.rs:118-130).
@@ -79,7 +95,7 @@ __device__ __forceinline__ void tunnel_controls(const BatchParams& p, const Batc
   target = T.u_ref * v1;
 }
 
-template <class S>
+template <class S, int STAGED>
 __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                        S* __restrict__ B) {
   using R = typename Store<S>::R;
@@ -91,23 +107,48 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
   const int nx = T.nx, ny = T.ny;
   const int x = td.z + (int)(threadIdx.x & ((1u << p.log2_tx) - 1u));
   const int y = td.y + (int)(threadIdx.x >> p.log2_tx);
-  if (x >= nx || y >= ny) return;
+  const bool in = x < nx && y < ny;
+  if (!STAGED && !in) return;
   const S* a = A + T.pop_off;
   S* b = B + T.pop_off;
   const unsigned idx = (unsigned)(y * nx + x);
-  const uint8_t fl = __ldg(p.flag + T.cell_off + idx);
+  int gfirst = 0;
+  if (STAGED && in) gfirst = __ldg(p.seg_bfirst + T.seg_off + y * T.segs + (x >> 5));
+  const uint8_t fl = in ? __ldg(p.flag + T.cell_off + idx) : (uint8_t)2;
   R f[9];
-  pull(a, T.ns, nx, ny, x, y, f);
+  if (in) pull(a, T.ns, nx, ny, x, y, f);
+  int g = -1;
+  if (STAGED) {
+    const unsigned bal = __ballot_sync(0xffffffffu, fl == 1);
+    if (!in) return;
+    g = gfirst + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+    if (fl == 1 && g < T.b_off + T.nb) {
+      const int2 dsc = __ldg(p.bdesc + g);
+      const R* __restrict__ lb = (const R*)p.lb;
+#pragma unroll
+      for (int d = 1; d < 9; ++d) {
+        const int j = opp_of(d);
+        if ((dsc.y >> j) & 1) f[d] = __ldg(lb + dsc.x + __popc((unsigned)dsc.y & ((1u << j) - 1u)));
+      }
+    }
+  }
   if (T.coll == COLL_BGK)
     collide_bgk(f, (R)T.op);
   else
     collide_trt(f, (R)T.op, (R)T.om);
-  if (fl != 0) return;
+  if (fl > (STAGED ? 1 : 0)) return;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * T.ns + idx, i, f[i]);
+  if (STAGED && fl == 1 && g < T.b_off + T.nb) {
+    S* __restrict__ oc = (S*)p.ownc;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Store<S>::st(oc + (unsigned)i * p.nbs + (unsigned)g, i, f[i]);
+  }
 }
 
-template <class S>
+// STAGED = 1: the link rules only (k_links_stage for a chunk): own populations from the compact
+// copy, the returning populations to the per-link array, no pull, collision or store.
+template <class S, int STAGED>
 __global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
   using R = typename Store<S>::R;
@@ -132,7 +173,16 @@ __global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ 
   if (cd.w == T.chunk_off && tid == 0 && !p.dry) st->drho = drho;
   s_acc[0][tid] = 0.0;
   s_acc[1][tid] = 0.0;
-  if (tid < cd.z) {
+  if (tid < cd.z && STAGED) {
+    const int g = cd.y + tid;
+    const S* __restrict__ oc = (const S*)p.ownc;
+    R own[9];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(oc + (unsigned)d * p.nbs + (unsigned)g, d);
+    R* __restrict__ lb = (R*)p.lb;
+    link_rules<S>(a, T.ns, own, __ldg(p.bnode_first + g), __ldg(p.bnode_first + g + 1), (const LinkRecDev*)p.links,
+                  vs, drho, 0.0, 0.0, p.sqrt_cs2, &s_acc[0][tid], [&](int l, int, R back) { lb[l] = back; });
+  } else if (tid < cd.z) {
     const int g = cd.y + tid;
     const int idx = __ldg(p.bnode_idx + g);
     R f[9];
@@ -169,6 +219,21 @@ __global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ 
     st->arrive = 0;
     __threadfence();
   }
+}
+
+// The compact copy of the boundary nodes' own populations of the chunks' tunnels, gathered from
+// `a` (one block per link chunk).
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_batch_gather_own(const __grid_constant__ BatchParams p, const S* __restrict__ A) {
+  const int4 cd = __ldg(p.chunks + blockIdx.x);
+  if ((int)threadIdx.x >= cd.z) return;
+  const BatchTunnel& T = p.tun[cd.x];
+  const int g = cd.y + (int)threadIdx.x;
+  const unsigned idx = (unsigned)__ldg(p.bnode_idx + g);
+  const S* a = A + T.pop_off;
+  S* oc = (S*)p.ownc;
+#pragma unroll
+  for (int d = 0; d < 9; ++d) oc[(unsigned)d * p.nbs + (unsigned)g] = a[(unsigned)d * T.ns + idx];
 }
 
 }  // namespace vl

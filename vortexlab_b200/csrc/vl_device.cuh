@@ -12,9 +12,18 @@
 //            row tile, grid-stride over tiles.
 //
 // Both read only `a` and write disjoint cells of `b`, so their order does not matter; the
-// whole-step epilogue runs in whichever block of the two launches arrives last (a counter in
-// device memory, no spin-waits): it reduces the per-block force partials in a fixed order, writes
-// the per-step record, evaluates the pressure-drop probes on the new state and advances t.
+// whole-step epilogue runs in the last link block to finish (a counter in device memory, no
+// spin-waits): it reduces the per-block force partials in a fixed order, writes the per-step
+// record, evaluates the pressure-drop probe of the previous step and advances t.
+//
+// The staged step is the other pairing: k_links_stage applies the link rules only and writes the
+// population each link returns into the fluid to a compact array (link order); then
+// k_bulk<S, CK, 1> updates every fluid cell of its row tiles, boundary cells included, taking
+// those populations in place of the pulled ones, and also writes the new populations of each
+// boundary node to a compact copy in CSR order, which the next k_links_stage reads instead of
+// `a`. The boundary cells then cost coalesced traffic instead of nine scattered 32-byte sectors
+// per store, per pull and per own value; the two kernels must run in that order. Both pairings
+// compute every population with the same expressions.
 //
 // Determinism: every population update is a pure function of `a`; the force is summed per thread
 // in link order, then by a fixed warp-shuffle tree, a fixed shared-memory tree and a fixed tree
@@ -80,6 +89,19 @@ struct StepParams {
   Ctl* ctl;
   double* partials;            // [nlink][2 * kMaxGroups]
   int ngroups;
+  // Staged step only: per boundary node (CSR order) {first link, bit j set for each link
+  // direction j}; per 32-cell warp slot of the bulk grid, the boundary nodes before its first cell;
+  // the population each link sends back into the fluid (arithmetic type, link order); the
+  // boundary nodes' own populations of the current state (stored type, 9 planes of stride nbs, CSR
+  // order), written by the staged bulk kernel beside `b` for the next step.
+  const int2* bdesc;
+  const int32_t* warp_bfirst;
+  void* lb;
+  void* ownc;
+  unsigned nbs;
+  // Launch ranges of the staged kernels (a step may launch each in two parts): link blocks
+  // [link_b0, link_b0 + link_n) and bulk tiles [bulk_b0, bulk_b0 + bulk_n), clipped to the grid.
+  int link_b0, link_n, bulk_b0, bulk_n;
 };
 
 struct alignas(16) LinkRecDev {
@@ -327,18 +349,44 @@ __device__ __forceinline__ void pull(const S* __restrict__ a, unsigned ns, int n
   f[8] = Store<S>::ld(a + 8u * ns + rp + xm, 8);
 }
 
-template <class S, int CK>
+//
+// STAGED = 1 (the staged step): the tile also updates its boundary cells (flag 1). Their pulled
+// populations come from the same coalesced row loads; each one that arrives across a link is
+// replaced by the value k_links_stage computed for that link, found through the node's descriptor:
+// the node's rank k in the CSR list is the warp's first rank plus the boundary cells before the
+// lane (a ballot), and the link of direction j is `first + popc(mask below j)` (the links of a node
+// are stored by ascending direction). Every fluid cell of the row is then written by this kernel.
+template <class S, int CK, int STAGED>
 __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepParams p,
                                                  const S* __restrict__ a, S* __restrict__ b) {
   using R = typename Store<S>::R;
   const int nx = p.nx, ny = p.ny;
-  const int y = blockIdx.x / p.tiles_per_row;
-  const int x = (blockIdx.x - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
-  if (x >= nx) return;
+  const int tile = (int)blockIdx.x + (STAGED ? p.bulk_b0 : 0);
+  const int y = tile / p.tiles_per_row;
+  const int x = (tile - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
+  if (!STAGED && x >= nx) return;
+  const bool in = x < nx;
   const unsigned idx = (unsigned)(y * nx + x);
-  const uint8_t fl = __ldg(p.flag + idx);
+  int wfirst = 0;
+  if (STAGED) wfirst = __ldg(p.warp_bfirst + (size_t)tile * (kBlock / 32) + (threadIdx.x >> 5));
+  const uint8_t fl = in ? __ldg(p.flag + idx) : (uint8_t)2;
   R f[9];
-  pull(a, p.ns, nx, ny, x, y, f);
+  if (in) pull(a, p.ns, nx, ny, x, y, f);
+  int k = -1;
+  if (STAGED) {
+    const unsigned bal = __ballot_sync(0xffffffffu, fl == 1);
+    if (!in) return;
+    k = wfirst + __popc(bal & ((1u << (threadIdx.x & 31)) - 1u));
+    if (fl == 1 && k < p.nb) {
+      const int2 dsc = __ldg(p.bdesc + k);
+      const R* __restrict__ lb = (const R*)p.lb;
+#pragma unroll
+      for (int d = 1; d < 9; ++d) {
+        const int j = opp_of(d);
+        if ((dsc.y >> j) & 1) f[d] = __ldg(lb + dsc.x + __popc((unsigned)dsc.y & ((1u << j) - 1u)));
+      }
+    }
+  }
   const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
   if (CK == 2)
     collide_forced(f, op, om, gx, gy);
@@ -346,9 +394,14 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepPar
     collide_bgk(f, op);
   else
     collide_trt(f, op, om);
-  if (fl != 0) return;
+  if (fl > (STAGED ? 1 : 0)) return;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * p.ns + idx, i, f[i]);
+  if (STAGED && fl == 1 && k < p.nb) {
+    S* __restrict__ oc = (S*)p.ownc;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Store<S>::st(oc + (unsigned)i * p.nbs + (unsigned)k, i, f[i]);
+  }
 }
 
 // ------------------------------------------------------------------ link kernel
@@ -412,10 +465,103 @@ __device__ double outlet_offset(const S* __restrict__ a, unsigned ns, const int3
   return s_drho;
 }
 
-// The link pass for one boundary node (src/sim.rs:456-503): the incoming populations (pulled
-// from the neighbours), each population that would come out of the boundary replaced by the rule
-// of its link, the momentum exchanged with each force group added to `acc` (component c at
-// acc[c * kBlock]), then the collision. `f` returns the post-collision populations.
+// The link rules of one boundary node (src/sim.rs:462-495): for link l with direction j, the
+// population `back` that returns into direction i = opp(j) is handed to put(l, i, back), and the
+// momentum exchanged with the link's force group is added to `acc` (component c at acc[c * kBlock]).
+// Every per-link read of the reference's link pass other than the node behind the link (a[j][idx],
+// a[i][idx], the node velocity) is one of the node's own post-collision populations `own`, so the
+// loop touches memory only for its record and that one node.
+// Whether a link's rule reads the node behind it: a wall link with q < 1/2 and a fluid node
+// behind (src/sim.rs:474-477).
+__device__ __forceinline__ bool uses_behind(const LinkView& L) {
+  return !(L.flags & 1) && L.q < 0.5 && L.behind >= 0;
+}
+
+// The returning population of one link. `bval` is a[j][behind] (read by the caller, so that it
+// can be loaded together with other links' values; any value when the rule does not use it).
+template <class S>
+__device__ __forceinline__ typename Store<S>::R link_back(typename Store<S>::R bval, const LinkView& L,
+                                                          const typename Store<S>::R* own, const double* vs,
+                                                          double drho, typename Store<S>::R gx,
+                                                          typename Store<S>::R gy, double sqrt_cs2, bool& have_u,
+                                                          typename Store<S>::R& ux, typename Store<S>::R& uy,
+                                                          typename Store<S>::R& out, typename Store<S>::R& scale) {
+  using R = typename Store<S>::R;
+  const int j = L.dir;
+  const int i = opp_of(j);
+  out = pick(own, j);
+  scale = (R)vs[L.vgroup];
+  R back;
+  if (!(L.flags & 1)) {
+    // Wall: interpolated bounce-back with the moving-wall term (src/sim.rs:467-479).
+    const R corr = (R)L.cu6 * scale;
+    const R q = (R)L.q;
+    if (q >= R(0.5)) {
+      const R kq = R(0.5) / q;
+      back = kq * (out - corr) + (R(1.0) - kq) * pick(own, i);
+    } else if (L.behind >= 0) {
+      back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * bval - corr;
+    } else {
+      back = out - corr;
+    }
+  } else {
+    // Open boundary: anti-bounce-back around the equilibrium of the boundary density
+    // (src/sim.rs:480-488), with the node's own velocity.
+    if (!have_u) {
+      R rho, jx, jy;
+      moments(own, rho, jx, jy);
+      ux = jx / rho - R(0.5) * gx;
+      uy = jy / rho - R(0.5) * gy;
+      have_u = true;
+    }
+    const R cu = R(3.0) * ((R)cx_of(j) * ux + (R)cy_of(j) * uy);
+    R rho_w;
+    if (L.flags & 2) {
+      const R nxv = (R)((int)((L.flags >> 2) & 3) - 1), nyv = (R)((int)((L.flags >> 4) & 3) - 1);
+      rho_w = (R)L.rho + (nxv * ux + nyv * uy) / (R)sqrt_cs2;
+    } else {
+      rho_w = (R)L.rho + (R)drho;
+    }
+    back = -out + R(2.0) * (R)w_of(j) * rho_w * (R(1.0) + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy));
+  }
+  return back;
+}
+
+// Galilean-invariant momentum exchange of one link (src/sim.rs:490-495), in FP64.
+__device__ __forceinline__ void force_terms(const LinkView& L, double o, double bk, double scale, double& tx,
+                                            double& ty) {
+  const double wux = L.uw0 * scale, wuy = L.uw1 * scale;
+  tx = (double)cx_of(L.dir) * (o + bk) - wux * (o - bk);
+  ty = (double)cy_of(L.dir) * (o + bk) - wuy * (o - bk);
+}
+
+template <class S, class Put>
+__device__ __forceinline__ void link_rules(const S* __restrict__ a, unsigned ns, const typename Store<S>::R* own,
+                                           int first, int last, const LinkRecDev* __restrict__ links,
+                                           const double* vs, double drho, double gx_, double gy_, double sqrt_cs2,
+                                           double* acc, Put put) {
+  using R = typename Store<S>::R;
+  const R gx = (R)gx_, gy = (R)gy_;
+  bool have_u = false;
+  R ux = R(0), uy = R(0);
+  for (int l = first; l < last; ++l) {
+    const LinkView L = load_link(links, l);
+    R out, scale;
+    const R bval = uses_behind(L) ? Store<S>::ld(a + (unsigned)L.dir * ns + (unsigned)L.behind, L.dir) : R(0);
+    const R back = link_back<S>(bval, L, own, vs, drho, gx, gy, sqrt_cs2, have_u, ux, uy, out, scale);
+    put(l, opp_of(L.dir), back);
+    if (L.fgroup >= 0) {
+      double tx, ty;
+      force_terms(L, (double)out, (double)back, (double)scale, tx, ty);
+      acc[(2 * L.fgroup) * kBlock] += tx;
+      acc[(2 * L.fgroup + 1) * kBlock] += ty;
+    }
+  }
+}
+
+// The link pass for one boundary node (src/sim.rs:456-503): the incoming populations pulled from
+// the neighbours, each one that would come out of the boundary replaced by its link's rule, then
+// the collision. `f` returns the post-collision populations.
 template <class S>
 __device__ __forceinline__ void link_node(const S* __restrict__ a, unsigned ns, int nx, int ny, int idx, int first,
                                           int last, const LinkRecDev* __restrict__ links, const double* vs,
@@ -424,64 +570,12 @@ __device__ __forceinline__ void link_node(const S* __restrict__ a, unsigned ns, 
   using R = typename Store<S>::R;
   const R op = (R)op_, om = (R)om_, gx = (R)gx_, gy = (R)gy_;
   const int y = idx / nx, x = idx - y * nx;
-  // The incoming populations and the node's own post-collision populations: every per-link read
-  // of the reference's link pass other than the node behind the link (a[j][idx], a[i][idx], the
-  // node velocity) is one of the own values, so the link loop touches memory only for its record
-  // and that one node.
   R own[9];
   pull(a, ns, nx, ny, x, y, f);
 #pragma unroll
   for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
-  bool have_u = false;
-  R ux = R(0), uy = R(0);
-  for (int l = first; l < last; ++l) {
-    const LinkView L = load_link(links, l);
-    const int j = L.dir;
-    const int i = opp_of(j);
-    const R out = pick(own, j);
-    const R scale = (R)vs[L.vgroup];
-    R back;
-    if (!(L.flags & 1)) {
-      // Wall: interpolated bounce-back with the moving-wall term (src/sim.rs:467-479).
-      const R corr = (R)L.cu6 * scale;
-      const R q = (R)L.q;
-      if (q >= R(0.5)) {
-        const R kq = R(0.5) / q;
-        back = kq * (out - corr) + (R(1.0) - kq) * pick(own, i);
-      } else if (L.behind >= 0) {
-        back = R(2.0) * q * out + (R(1.0) - R(2.0) * q) * Store<S>::ld(a + (unsigned)j * ns + (unsigned)L.behind, j) - corr;
-      } else {
-        back = out - corr;
-      }
-    } else {
-      // Open boundary: anti-bounce-back around the equilibrium of the boundary density
-      // (src/sim.rs:480-488), with the node's own velocity.
-      if (!have_u) {
-        R rho, jx, jy;
-        moments(own, rho, jx, jy);
-        ux = jx / rho - R(0.5) * gx;
-        uy = jy / rho - R(0.5) * gy;
-        have_u = true;
-      }
-      const R cu = R(3.0) * ((R)cx_of(j) * ux + (R)cy_of(j) * uy);
-      R rho_w;
-      if (L.flags & 2) {
-        const R nxv = (R)((int)((L.flags >> 2) & 3) - 1), nyv = (R)((int)((L.flags >> 4) & 3) - 1);
-        rho_w = (R)L.rho + (nxv * ux + nyv * uy) / (R)sqrt_cs2;
-      } else {
-        rho_w = (R)L.rho + (R)drho;
-      }
-      back = -out + R(2.0) * (R)w_of(j) * rho_w * (R(1.0) + R(0.5) * cu * cu - R(1.5) * (ux * ux + uy * uy));
-    }
-    set_dir(f, i, back);
-    if (L.fgroup >= 0) {
-      // Galilean-invariant momentum exchange (src/sim.rs:490-495), accumulated in FP64.
-      const double o = (double)out, bk = (double)back;
-      const double wux = L.uw0 * (double)scale, wuy = L.uw1 * (double)scale;
-      acc[(2 * L.fgroup) * kBlock] += (double)cx_of(j) * (o + bk) - wux * (o - bk);
-      acc[(2 * L.fgroup + 1) * kBlock] += (double)cy_of(j) * (o + bk) - wuy * (o - bk);
-    }
-  }
+  link_rules<S>(a, ns, own, first, last, links, vs, drho, gx_, gy_, sqrt_cs2, acc,
+                [&](int, int i, R back) { set_dir(f, i, back); });
   if (ck == 2)
     collide_forced(f, op, om, gx, gy);
   else if (ck == 0)
@@ -540,6 +634,56 @@ __global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links(const __gr
     block_force_partial(s_acc, ncomp, p.partials + (size_t)blockIdx.x * (2 * kMaxGroups));
   }
   arrive<S>(p, a);
+}
+
+// First kernel of the staged step: the link rules of every boundary node, without the pull, the
+// collision or the store (k_bulk<S, CK, 1> does those in its row tiles). Writes the returning
+// population of each link to p.lb in link order; force partials, outlet offset and the end-of-step
+// epilogue as k_links (the arrival count spans both parts when the kernel is launched in two). The
+// node's own populations come from the compact copy p.ownc (the same stored values as `a`), so the
+// node behind a link is the only scattered read. Blocks are numbered from p.link_b0.
+template <class S>
+__global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links_stage(const __grid_constant__ StepParams p,
+                                                                          const S* __restrict__ a) {
+  using R = typename Store<S>::R;
+  __shared__ double s_un[kBlock];
+  __shared__ double s_acc[2 * kMaxGroups][kBlock];
+  const int tid = threadIdx.x;
+  const Controls ctl = read_controls(p.ctl);
+  const double drho = (ctl.has_target && p.np > 0)
+                          ? outlet_offset(a, p.ns, p.pnode_idx, p.pnode_n, p.np, p.gx, p.gy, ctl.target, p.sqrt_cs2, s_un)
+                          : 0.0;
+  if (blockIdx.x + p.link_b0 == 0 && tid == 0 && !p.ctl->dry) p.ctl->drho = drho;
+  const int ncomp = 2 * p.ngroups;
+  for (int c = 0; c < ncomp; ++c) s_acc[c][tid] = 0.0;
+  const int blk = (int)blockIdx.x + p.link_b0;
+  const int k = blk * kBlock + tid;
+  if (k < p.nb) {
+    const S* __restrict__ oc = (const S*)p.ownc;
+    R own[9];
+#pragma unroll
+    for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(oc + (unsigned)d * p.nbs + (unsigned)k, d);
+    R* __restrict__ lb = (R*)p.lb;
+    link_rules<S>(a, p.ns, own, __ldg(p.bnode_first + k), __ldg(p.bnode_first + k + 1), (const LinkRecDev*)p.links,
+                  ctl.vs, drho, p.gx, p.gy, p.sqrt_cs2, &s_acc[0][tid], [&](int l, int, R back) { lb[l] = back; });
+  }
+  if (ncomp > 0) {
+    __syncthreads();
+    block_force_partial(s_acc, ncomp, p.partials + (size_t)blk * (2 * kMaxGroups));
+  }
+  arrive<S>(p, a);
+}
+
+// The compact copy of the boundary nodes' own populations read by k_links_stage, gathered from `a`
+// whenever the state was set other than by a staged step (init, upload, another schedule).
+template <class S>
+__global__ void k_gather_own(int nb, unsigned ns, unsigned nbs, const int32_t* __restrict__ bidx,
+                             const S* __restrict__ a, S* __restrict__ oc) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nb; k += gridDim.x * blockDim.x) {
+    const unsigned idx = (unsigned)__ldg(bidx + k);
+#pragma unroll
+    for (int d = 0; d < 9; ++d) oc[(unsigned)d * nbs + (unsigned)k] = a[(unsigned)d * ns + idx];
+  }
 }
 
 // ------------------------------------------------------------------ utility kernels

@@ -14,7 +14,9 @@ struct BatchParams;
 
 struct Launchers {
   size_t elem;  // bytes per stored population value
-  // One step: the link kernel then the bulk kernel, both on `s`. ck: 0 BGK, 1 TRT, 2 forced.
+  // One step: the link kernel then the bulk kernel, both on `s`. ck: 0 BGK, 1 TRT, 2 forced, plus
+  // 0x100 link kernel only, 0x200 bulk kernel only, 0x400 the staged pair (k_links_stage, then the
+  // bulk kernel that also updates boundary cells).
   cudaError_t (*step)(const StepParams& p, int ck, const void* a, void* b, cudaStream_t s);
   cudaError_t (*init)(int n, unsigned ns, const uint8_t* flag, const double* rho, const double* ux,
                       const double* uy, double rho0, double ux0, double uy0, void* a, void* b, cudaStream_t s);
@@ -30,9 +32,14 @@ struct Launchers {
   cudaError_t (*gather)(int m, unsigned ns, const int32_t* cells, const void* a, double* out, cudaStream_t s);
   // Records the pressure probe of the last step of a batch (one block).
   cudaError_t (*probe)(const StepParams& p, const void* a, cudaStream_t s);
-  // One step of a batch of tunnels: which = 1 link kernel, 2 bulk kernel, 3 both.
+  // One step of a batch of tunnels: which = 1 link kernel, 2 bulk kernel, 3 both; + 4 the staged
+  // pair (link rules only, then the bulk kernel that also updates boundary cells).
   cudaError_t (*batch_step)(const BatchParams& p, int ntiles, int nchunks, int which, const void* a, void* b,
                             cudaStream_t s);
+  // Gathers the boundary nodes' own populations of `a` into the staged step's compact copy.
+  cudaError_t (*gather_own)(const StepParams& p, const void* a, cudaStream_t s);
+  // The same for the tunnels of a batch's current link chunks.
+  cudaError_t (*batch_gather_own)(const BatchParams& p, int nchunks, const void* a, cudaStream_t s);
 };
 
 // Records a failure for vl_last_error / vl_last_status (thread-local) and returns `code`.

@@ -10,23 +10,30 @@ namespace vl {
 template <class S>
 struct LaunchImpl {
   // which: 3 = both kernels of the step, 1 = the link kernel only, 2 = the bulk kernel only
-  // (a step launched in two halves, for per-kernel timing).
+  // (a step launched in two halves, for per-kernel timing). staged: the link-values kernel and the
+  // bulk kernel that also updates the boundary cells, which must run in that order.
   template <int CK>
-  static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which) {
-    if (which & 1) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
-    if (which & 2) k_bulk<S, CK><<<p.nbulk, kBlock, 0, s>>>(p, a, b);
+  static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which, bool staged) {
+    if (staged) {
+      if (which & 1) k_links_stage<S><<<p.nlink - p.link_b0 < p.link_n ? p.nlink - p.link_b0 : p.link_n, kBlock, 0, s>>>(p, a);
+      if (which & 2) k_bulk<S, CK, 1><<<p.nbulk - p.bulk_b0 < p.bulk_n ? p.nbulk - p.bulk_b0 : p.bulk_n, kBlock, 0, s>>>(p, a, b);
+    } else {
+      if (which & 1) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
+      if (which & 2) k_bulk<S, CK, 0><<<p.nbulk, kBlock, 0, s>>>(p, a, b);
+    }
     return cudaGetLastError();
   }
   // ck: collision kind (0 BGK, 1 TRT, 2 forced) in the low byte; bit 8 = link kernel only,
-  // bit 9 = bulk kernel only.
+  // bit 9 = bulk kernel only, bit 10 = the staged pair.
   static cudaError_t step(const StepParams& p, int ck, const void* a, void* b, cudaStream_t s) {
     const S* A = (const S*)a;
     S* B = (S*)b;
     const int which = (ck & 0x300) ? ((ck & 0x100) ? 1 : 0) | ((ck & 0x200) ? 2 : 0) : 3;
+    const bool staged = (ck & 0x400) != 0;
     switch (ck & 0xff) {
-      case 0: return step_ck<0>(p, A, B, s, which);
-      case 2: return step_ck<2>(p, A, B, s, which);
-      default: return step_ck<1>(p, A, B, s, which);
+      case 0: return step_ck<0>(p, A, B, s, which, staged);
+      case 2: return step_ck<2>(p, A, B, s, which, staged);
+      default: return step_ck<1>(p, A, B, s, which, staged);
     }
   }
   static int grid_for(int n) { return n <= 0 ? 1 : (n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16; }
@@ -67,14 +74,31 @@ struct LaunchImpl {
     k_probe<S><<<1, kBlock, 0, s>>>(p, (const S*)a);
     return cudaGetLastError();
   }
+  // which: 1 link kernel, 2 bulk kernel, 3 both; + 4 the staged pair.
   static cudaError_t batch_step(const BatchParams& p, int ntiles, int nchunks, int which, const void* a, void* b,
                                 cudaStream_t s) {
-    if ((which & 1) && nchunks > 0) k_batch_links<S><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
-    if ((which & 2) && ntiles > 0) k_batch_bulk<S><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+    if (which & 4) {
+      if ((which & 1) && nchunks > 0) k_batch_links<S, 1><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      if ((which & 2) && ntiles > 0) k_batch_bulk<S, 1><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+    } else {
+      if ((which & 1) && nchunks > 0) k_batch_links<S, 0><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      if ((which & 2) && ntiles > 0) k_batch_bulk<S, 0><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+    }
+    return cudaGetLastError();
+  }
+  static cudaError_t batch_gather_own(const BatchParams& p, int nchunks, const void* a, cudaStream_t s) {
+    if (nchunks <= 0) return cudaSuccess;
+    k_batch_gather_own<S><<<nchunks, kBlock, 0, s>>>(p, (const S*)a);
+    return cudaGetLastError();
+  }
+  static cudaError_t gather_own(const StepParams& p, const void* a, cudaStream_t s) {
+    if (p.nb <= 0) return cudaSuccess;
+    k_gather_own<S><<<grid_for(p.nb), 256, 0, s>>>(p.nb, p.ns, p.nbs, p.bnode_idx, (const S*)a, (S*)p.ownc);
     return cudaGetLastError();
   }
   static const Launchers& table() {
-    static const Launchers t = {sizeof(S), &step, &init, &init_grid, &to_f64, &from_f64, &macros, &reduce, &gather, &probe, &batch_step};
+    static const Launchers t = {sizeof(S), &step, &init, &init_grid, &to_f64, &from_f64, &macros, &reduce, &gather, &probe, &batch_step,
+                                &gather_own, &batch_gather_own};
     return t;
   }
 };
