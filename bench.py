@@ -30,8 +30,9 @@ FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per node update of the bulk kernel from ncu (dram__bytes_read.sum +
 # dram__bytes_write.sum of one launch of the 2048 x 2048 box divided by the nodes it updates:
 # interior nodes for the two-kernel step, all fluid nodes for the staged step; see
-# profiles/k_bulk_k_links_f64_disk_box.md), per (precision, staged). Scaled to a full launch by nodes.
-NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3}
+# profiles/k_bulk_k_links_f64_disk_box.md and profiles/k_links_stage_k_bulk_staged_f64_disk_box.md),
+# per (precision, staged). Scaled to a full launch by nodes.
+NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3, ("f64", True): 140.2}
 
 
 def workload_name(prec):
@@ -270,7 +271,8 @@ def run_vortexlab(args):
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
                 "traffic": None if traffic is None else round(traffic * bulk_nodes),
-                "kernel": "k_bulk (staged: all fluid nodes)" if staged else "k_bulk (interior nodes)",
+                "kernel": ("k_bulk (staged: all fluid nodes; both launches of a step, with the second link "
+                           "part beside them)") if staged else "k_bulk (interior nodes)",
                 "algorithmic_bytes_per_launch": bulk_nodes * bpl,
                 "kernel_ms_per_launch": round(bulk_ms / args.steps, 4),
                 "link_kernel_ms_per_launch": round(link_ms / args.steps, 4),

@@ -156,8 +156,10 @@ def test_graph_and_single_steps_agree(gpu):
 
 
 def test_schedules_and_autotune_do_not_change_results(gpu):
-    """The four step schedules give bit-identical states and force histories; autotuning (dry-run
-    timing) leaves t, the force, the history and the state untouched."""
+    """The four step schedules give bit-identical states; the force histories are bit-identical
+    for the three two-kernel schedules, and equal to rounding for the staged step (which sums the
+    force terms per block of links, another fixed order). Autotuning (dry-run timing) leaves t, the
+    force, the history and the state untouched."""
     V = gpu
     results = []
     for sched in ("concurrent", "links-first", "bulk-first", "staged", "auto"):
@@ -173,8 +175,13 @@ def test_schedules_and_autotune_do_not_change_results(gpu):
         else:
             sim.schedule = sched
         r.ch.step(150)
-        results.append((sim.state_hash(), sim.history().tobytes()))
-    assert all(x == results[0] for x in results)
+        results.append((sched, sim.schedule, sim.state_hash(), sim.history()))
+    for sched, used, h, hist in results:
+        assert h == results[0][2], sched
+        if used == "staged":
+            assert np.max(np.abs(hist - results[0][3])) <= 1e-13 * np.max(np.abs(results[0][3])), sched
+        else:
+            assert np.array_equal(hist, results[0][3]), sched
 
 
 @pytest.mark.parametrize("n", [20, 40, 80])
@@ -283,5 +290,6 @@ def test_staged_schedule_follows_every_change_of_state(gpu):
         sim.step(9)
         sim.init((1.0, 0.02, -0.01))      # re-initialised
         sim.step(12)
-        out.append((sim.state_hash(), sim.force.tobytes()))
-    assert out[0] == out[1]
+        out.append((sim.state_hash(), sim.force.copy()))
+    assert out[0][0] == out[1][0]
+    assert _force_close(out[1][1], out[0][1], rel=1e-13)

@@ -79,6 +79,7 @@ struct vl_sim {
   double* d_gather = nullptr;
   int2* d_bdesc = nullptr;         // staged step: per boundary node {first link, link-direction mask}
   int32_t* d_wbfirst = nullptr;    // staged step: boundary nodes before each 32-cell warp slot
+  int32_t* d_lnode = nullptr;      // staged step: boundary node of each link
   void* d_lb = nullptr;            // staged step: returning population per link
   void* d_ownc = nullptr;          // staged step: boundary nodes' own populations (CSR order)
   bool own_ok = false;             // d_ownc holds the boundary nodes of the current state
@@ -107,7 +108,7 @@ struct vl_sim {
     if (device >= 0) cudaSetDevice(device);
     if (gexec) cudaGraphExecDestroy(gexec);
     void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_ctl,
-                    d_partials, d_hist, d_sched, d_red, d_cells, d_gather, d_bdesc, d_wbfirst, d_lb, d_ownc};
+                    d_partials, d_hist, d_sched, d_red, d_cells, d_gather, d_bdesc, d_wbfirst, d_lb, d_ownc, d_lnode};
     for (void* p : ptrs)
       if (p) cudaFree(p);
     for (cudaEvent_t e : pev) cudaEventDestroy(e);
@@ -184,7 +185,7 @@ struct vl_sim {
     pa.bulk_b0 = 0;
     pa.bulk_n = split_tiles;
     pb.link_b0 = split_links;
-    pb.link_n = P.nlink - split_links;
+    pb.link_n = P.nlinkblk - split_links;
     pb.bulk_b0 = split_tiles;
     pb.bulk_n = P.nbulk - split_tiles;
     const int lk = ck | 0x100 | 0x400, bk = ck | 0x200 | 0x400;
@@ -476,6 +477,10 @@ bool staged_tables(const vl::CompiledDomain& d, int tiles_per_row, std::vector<i
   return true;
 }
 
+#ifndef VL_STAGE_SPLIT
+#define VL_STAGE_SPLIT 4
+#endif
+
 // Creates the device-resident sim for a compiled domain.
 vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   int ndev = 0;
@@ -570,7 +575,10 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.np = (int)d.pnode_idx.size();
   P.ctl = s->d_ctl;
   P.ngroups = d.ngroups;
-  if (!chk(alloc_copy((void**)&s->d_partials, nullptr, (size_t)P.nlink * 2 * vl::kMaxGroups * sizeof(double))))
+  P.nlinks = (int)d.links.size();
+  P.nlinkblk = std::max(1, (P.nlinks + vl::kBlock * vl::kStagePer - 1) / (vl::kBlock * vl::kStagePer));
+  if (!chk(alloc_copy((void**)&s->d_partials, nullptr,
+                      (size_t)std::max(P.nlink, P.nlinkblk) * 2 * vl::kMaxGroups * sizeof(double))))
     return nullptr;
   P.partials = s->d_partials;
   // Staged step: node descriptors, per-warp boundary ranks and the per-link output.
@@ -588,15 +596,21 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
     return nullptr;
   P.nbs = (unsigned)((nb + 63) / 64 * 64);
   if (!chk(alloc_copy(&s->d_ownc, nullptr, (size_t)P.nbs * 9 * s->L->elem))) return nullptr;
+  std::vector<int32_t> lnode(d.links.size());
+  for (int k = 0; k < nb; ++k)
+    for (int l = d.bnode_first[k]; l < d.bnode_first[k + 1]; ++l) lnode[(size_t)l] = k;
+  if (!chk(alloc_copy((void**)&s->d_lnode, lnode.data(), lnode.size() * sizeof(int32_t)))) return nullptr;
+  P.lnode = s->d_lnode;
   P.link_b0 = 0;
-  P.link_n = P.nlink;
+  P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
   P.bulk_n = P.nbulk;
-  // Split point of the staged step: a quarter of the link blocks, and the row tiles before the row
-  // of the first boundary node they leave to the second part.
-  if (P.nlink >= 4) {
-    const int la = P.nlink / 4;
-    const int row = d.bnode_idx[(size_t)la * vl::kBlock] / (int)d.nx;
+  // Split point of the staged step: a fraction 1 / VL_STAGE_SPLIT of the link blocks, and the row
+  // tiles before the row of the node of the first link they leave to the second part (every
+  // boundary node of the earlier rows has all its links in the first part).
+  if (P.nlinkblk >= VL_STAGE_SPLIT) {
+    const int la = P.nlinkblk / VL_STAGE_SPLIT;
+    const int row = d.bnode_idx[(size_t)lnode[(size_t)la * vl::kBlock * vl::kStagePer]] / (int)d.nx;
     if (row > 0) {
       s->split_links = la;
       s->split_tiles = row * P.tiles_per_row;

@@ -16,14 +16,16 @@
 // spin-waits): it reduces the per-block force partials in a fixed order, writes the per-step
 // record, evaluates the pressure-drop probe of the previous step and advances t.
 //
-// The staged step is the other pairing: k_links_stage applies the link rules only and writes the
-// population each link returns into the fluid to a compact array (link order); then
+// The staged step is the other pairing: k_links_stage applies the link rules only (one thread per
+// link) and writes the population each link returns into the fluid to a compact array (link
+// order); then
 // k_bulk<S, CK, 1> updates every fluid cell of its row tiles, boundary cells included, taking
 // those populations in place of the pulled ones, and also writes the new populations of each
 // boundary node to a compact copy in CSR order, which the next k_links_stage reads instead of
 // `a`. The boundary cells then cost coalesced traffic instead of nine scattered 32-byte sectors
 // per store, per pull and per own value; the two kernels must run in that order. Both pairings
-// compute every population with the same expressions.
+// compute every population with the same expressions (the staged step sums the force terms per
+// block of links rather than per node, a different fixed order: equal to rounding).
 //
 // Determinism: every population update is a pure function of `a`; the force is summed per thread
 // in link order, then by a fixed warp-shuffle tree, a fixed shared-memory tree and a fixed tree
@@ -99,8 +101,11 @@ struct StepParams {
   void* lb;
   void* ownc;
   unsigned nbs;
-  // Launch ranges of the staged kernels (a step may launch each in two parts): link blocks
-  // [link_b0, link_b0 + link_n) and bulk tiles [bulk_b0, bulk_b0 + bulk_n), clipped to the grid.
+  // Staged link kernel: one thread per link, nlinkblk blocks of kBlock links; lnode[l] = boundary
+  // node (CSR index) of link l. Launch ranges (a step may launch each kernel in two parts): link
+  // blocks [link_b0, link_b0 + link_n) and bulk tiles [bulk_b0, bulk_b0 + bulk_n), clipped.
+  const int32_t* lnode;
+  int nlinks, nlinkblk;
   int link_b0, link_n, bulk_b0, bulk_n;
 };
 
@@ -256,14 +261,14 @@ __device__ __forceinline__ double sum_partials(const double* v, int count, int s
 // writes the step record, evaluates the pressure probe of the previous step (whose result is the
 // current `a`), advances the controls and t.
 template <class S>
-__device__ void step_epilogue(const StepParams& p, const S* __restrict__ a) {
+__device__ void step_epilogue(const StepParams& p, const S* __restrict__ a, int nblocks) {
   __shared__ double red[kBlock];
   __shared__ double res[2 * kMaxGroups];
   const int tid = threadIdx.x;
   Ctl* c = p.ctl;
   const int ncomp = 2 * p.ngroups;
   for (int k = 0; k < ncomp; ++k) {
-    const double v = sum_partials(p.partials + k, p.nlink, 2 * kMaxGroups, red);
+    const double v = sum_partials(p.partials + k, nblocks, 2 * kMaxGroups, red);
     if (tid == 0) res[k] = v;
   }
   __syncthreads();
@@ -302,20 +307,21 @@ __device__ void step_epilogue(const StepParams& p, const S* __restrict__ a) {
   }
 }
 
-// Link blocks publish their force partial and count themselves; the last one runs the epilogue.
+// Link blocks publish their force partial and count themselves; the last of the step's `nblocks`
+// blocks runs the epilogue.
 template <class S>
-__device__ __forceinline__ void arrive(const StepParams& p, const S* __restrict__ a) {
+__device__ __forceinline__ void arrive(const StepParams& p, const S* __restrict__ a, int nblocks) {
   __shared__ int last;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
     const unsigned prev = atomicAdd(&p.ctl->arrive, 1u);
-    last = prev == (unsigned)(p.nlink - 1);
+    last = prev == (unsigned)(nblocks - 1);
   }
   __syncthreads();
   if (last) {
     __threadfence();
-    step_epilogue<S>(p, a);
+    step_epilogue<S>(p, a, nblocks);
   }
 }
 
@@ -633,18 +639,24 @@ __global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links(const __gr
     __syncthreads();
     block_force_partial(s_acc, ncomp, p.partials + (size_t)blockIdx.x * (2 * kMaxGroups));
   }
-  arrive<S>(p, a);
+  arrive<S>(p, a, p.nlink);
 }
 
-// First kernel of the staged step: the link rules of every boundary node, without the pull, the
-// collision or the store (k_bulk<S, CK, 1> does those in its row tiles). Writes the returning
-// population of each link to p.lb in link order; force partials, outlet offset and the end-of-step
-// epilogue as k_links (the arrival count spans both parts when the kernel is launched in two). The
-// node's own populations come from the compact copy p.ownc (the same stored values as `a`), so the
-// node behind a link is the only scattered read. Blocks are numbered from p.link_b0.
+#ifndef VL_STAGE_PER
+#define VL_STAGE_PER 1
+#endif
+constexpr int kStagePer = VL_STAGE_PER;  // links per thread of k_links_stage
+
+// First kernel of the staged step: the link rules of every link, without the pull, the collision
+// or the store (k_bulk<S, CK, 1> does those in its row tiles). kStagePer links per thread (blocks of
+// kBlock * kStagePer links, numbered from p.link_b0, p.nlinkblk in all), so each thread's loads
+// (record, the node's own populations from the compact copy p.ownc, the node behind) are one short
+// chain. Writes
+// the returning population of each link to p.lb; the force terms of the block's links go through
+// the fixed shuffle / shared-memory tree into the block partial, the last of the p.nlinkblk blocks
+// runs the end-of-step epilogue, the outlet offset is computed per block as in k_links.
 template <class S>
-__global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links_stage(const __grid_constant__ StepParams p,
-                                                                          const S* __restrict__ a) {
+__global__ void __launch_bounds__(kBlock) k_links_stage(const __grid_constant__ StepParams p, const S* __restrict__ a) {
   using R = typename Store<S>::R;
   __shared__ double s_un[kBlock];
   __shared__ double s_acc[2 * kMaxGroups][kBlock];
@@ -653,25 +665,68 @@ __global__ void __launch_bounds__(kBlock, VL_LINK_MIN_BLOCKS) k_links_stage(cons
   const double drho = (ctl.has_target && p.np > 0)
                           ? outlet_offset(a, p.ns, p.pnode_idx, p.pnode_n, p.np, p.gx, p.gy, ctl.target, p.sqrt_cs2, s_un)
                           : 0.0;
-  if (blockIdx.x + p.link_b0 == 0 && tid == 0 && !p.ctl->dry) p.ctl->drho = drho;
+  const int blk = (int)blockIdx.x + p.link_b0;
+  if (blk == 0 && tid == 0 && !p.ctl->dry) p.ctl->drho = drho;
   const int ncomp = 2 * p.ngroups;
   for (int c = 0; c < ncomp; ++c) s_acc[c][tid] = 0.0;
-  const int blk = (int)blockIdx.x + p.link_b0;
-  const int k = blk * kBlock + tid;
-  if (k < p.nb) {
-    const S* __restrict__ oc = (const S*)p.ownc;
-    R own[9];
+  // Links blk * kBlock * kStagePer + tid + m * kBlock (m < kStagePer): every record first, then
+  // every value the rules read, then the arithmetic, so the loads of all of a thread's links are in
+  // flight together. The thread adds its links' force terms in m order.
+  const LinkRecDev* __restrict__ links = (const LinkRecDev*)p.links;
+  const S* __restrict__ oc = (const S*)p.ownc;
+  const int lbase = blk * kBlock * kStagePer + tid;
+  LinkView L[kStagePer];
+  unsigned kn[kStagePer];
 #pragma unroll
-    for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(oc + (unsigned)d * p.nbs + (unsigned)k, d);
-    R* __restrict__ lb = (R*)p.lb;
-    link_rules<S>(a, p.ns, own, __ldg(p.bnode_first + k), __ldg(p.bnode_first + k + 1), (const LinkRecDev*)p.links,
-                  ctl.vs, drho, p.gx, p.gy, p.sqrt_cs2, &s_acc[0][tid], [&](int l, int, R back) { lb[l] = back; });
+  for (int m = 0; m < kStagePer; ++m) {
+    const int l = lbase + m * kBlock;
+    if (l < p.nlinks) {
+      kn[m] = (unsigned)__ldg(p.lnode + l);
+      L[m] = load_link(links, l);
+    }
+  }
+  R vj[kStagePer], vi[kStagePer], bv[kStagePer];
+#pragma unroll
+  for (int m = 0; m < kStagePer; ++m) {
+    const int l = lbase + m * kBlock;
+    if (l < p.nlinks) {
+      const int j = L[m].dir, i = opp_of(j);
+      vj[m] = Store<S>::ld(oc + (unsigned)j * p.nbs + kn[m], j);
+      vi[m] = Store<S>::ld(oc + (unsigned)i * p.nbs + kn[m], i);
+      bv[m] = uses_behind(L[m]) ? Store<S>::ld(a + (unsigned)j * p.ns + (unsigned)L[m].behind, j) : R(0);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < kStagePer; ++m) {
+    const int l = lbase + m * kBlock;
+    if (l < p.nlinks) {
+      const int j = L[m].dir, i = opp_of(j);
+      R own[9];
+      if (L[m].flags & 1) {
+#pragma unroll
+        for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(oc + (unsigned)d * p.nbs + kn[m], d);
+      } else {
+#pragma unroll
+        for (int d = 0; d < 9; ++d) own[d] = d == j ? vj[m] : (d == i ? vi[m] : R(0));
+      }
+      bool have_u = false;
+      R ux = R(0), uy = R(0), out, scale;
+      const R back =
+          link_back<S>(bv[m], L[m], own, ctl.vs, drho, (R)p.gx, (R)p.gy, p.sqrt_cs2, have_u, ux, uy, out, scale);
+      ((R*)p.lb)[l] = back;
+      if (L[m].fgroup >= 0) {
+        double tx, ty;
+        force_terms(L[m], (double)out, (double)back, (double)scale, tx, ty);
+        s_acc[2 * L[m].fgroup][tid] += tx;
+        s_acc[2 * L[m].fgroup + 1][tid] += ty;
+      }
+    }
   }
   if (ncomp > 0) {
     __syncthreads();
     block_force_partial(s_acc, ncomp, p.partials + (size_t)blk * (2 * kMaxGroups));
   }
-  arrive<S>(p, a);
+  arrive<S>(p, a, p.nlinkblk);
 }
 
 // The compact copy of the boundary nodes' own populations read by k_links_stage, gathered from `a`

@@ -15,7 +15,7 @@ struct LaunchImpl {
   template <int CK>
   static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which, bool staged) {
     if (staged) {
-      if (which & 1) k_links_stage<S><<<p.nlink - p.link_b0 < p.link_n ? p.nlink - p.link_b0 : p.link_n, kBlock, 0, s>>>(p, a);
+      if (which & 1) k_links_stage<S><<<p.nlinkblk - p.link_b0 < p.link_n ? p.nlinkblk - p.link_b0 : p.link_n, kBlock, 0, s>>>(p, a);
       if (which & 2) k_bulk<S, CK, 1><<<p.nbulk - p.bulk_b0 < p.bulk_n ? p.nbulk - p.bulk_b0 : p.bulk_n, kBlock, 0, s>>>(p, a, b);
     } else {
       if (which & 1) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
