@@ -83,7 +83,7 @@ struct vl_sim {
   void* d_lb = nullptr;            // staged step: returning population per link
   void* d_ownc = nullptr;          // staged step: boundary nodes' own populations (CSR order)
   bool own_ok = false;             // d_ownc holds the boundary nodes of the current state
-  int split_links = 0, split_tiles = 0;  // staged step in two parts (0: one part)
+  int split_links = 0, split_rows = 0;  // staged step in two parts (0: one part)
   cudaStream_t stream = nullptr;   // the sim's stream: bulk kernel, copies, everything else
   cudaStream_t aux = nullptr;      // the link kernel of each step, forked from and joined to `stream`
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -174,7 +174,7 @@ struct vl_sim {
   }
 
   // The staged step in two parts. The first `split_links` link blocks run first; then the bulk
-  // tiles of the rows whose boundary nodes they hold (`split_tiles` tiles), while the remaining link
+  // tiles of the rows whose boundary nodes they hold (`split_rows` rows), while the remaining link
   // blocks run beside them on `aux`; then the remaining tiles, after both. Only the first part of
   // the link kernel is exposed. The events bracket the exposed link part and the two bulk parts.
   cudaError_t enqueue_staged_split(cudaEvent_t lk0, cudaEvent_t lk1, cudaEvent_t bk0, cudaEvent_t bk1) {
@@ -183,11 +183,11 @@ struct vl_sim {
     pa.link_b0 = 0;
     pa.link_n = split_links;
     pa.bulk_b0 = 0;
-    pa.bulk_n = split_tiles;
+    pa.bulk_n = split_rows;
     pb.link_b0 = split_links;
     pb.link_n = P.nlinkblk - split_links;
-    pb.bulk_b0 = split_tiles;
-    pb.bulk_n = P.nbulk - split_tiles;
+    pb.bulk_b0 = split_rows;
+    pb.bulk_n = P.ny - split_rows;
     const int lk = ck | 0x100 | 0x400, bk = ck | 0x200 | 0x400;
     if ((e = cudaEventRecord(ev_fork, stream)) != cudaSuccess) return e;
     if ((e = cudaStreamWaitEvent(aux, ev_fork, 0)) != cudaSuccess) return e;
@@ -604,7 +604,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.link_b0 = 0;
   P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
-  P.bulk_n = P.nbulk;
+  P.bulk_n = P.ny;
   // Split point of the staged step: a fraction 1 / VL_STAGE_SPLIT of the link blocks, and the row
   // tiles before the row of the node of the first link they leave to the second part (every
   // boundary node of the earlier rows has all its links in the first part).
@@ -613,7 +613,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
     const int row = d.bnode_idx[(size_t)lnode[(size_t)la * vl::kBlock * vl::kStagePer]] / (int)d.nx;
     if (row > 0) {
       s->split_links = la;
-      s->split_tiles = row * P.tiles_per_row;
+      s->split_rows = row;
     }
   }
   P.bdesc = s->d_bdesc;

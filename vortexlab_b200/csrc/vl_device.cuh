@@ -8,8 +8,8 @@
 //            (src/sim.rs:456-507), accumulate the momentum-exchange force per force group,
 //            collide, write. One thread per boundary node of the CSR node list.
 //   k_bulk   interior nodes (flag 0): pull the 9 populations from the upstream neighbours with
-//            periodic wrap (src/sim.rs:700-735), collide, write. One thread per cell of a
-//            row tile, grid-stride over tiles.
+//            periodic wrap (src/sim.rs:700-735), collide, write. One thread per cell; one
+//            block per tile of kBlock cells of a row (grid x = tile of the row, y = row).
 //
 // Both read only `a` and write disjoint cells of `b`, so their order does not matter; the
 // whole-step epilogue runs in the last link block to finish (a counter in device memory, no
@@ -18,8 +18,7 @@
 //
 // The staged step is the other pairing: k_links_stage applies the link rules only (one thread per
 // link) and writes the population each link returns into the fluid to a compact array (link
-// order); then
-// k_bulk<S, CK, 1> updates every fluid cell of its row tiles, boundary cells included, taking
+// order); then k_bulk<S, CK, 1> updates every fluid cell of its row tiles, boundary cells included, taking
 // those populations in place of the pulled ones, and also writes the new populations of each
 // boundary node to a compact copy in CSR order, which the next k_links_stage reads instead of
 // `a`. The boundary cells then cost coalesced traffic instead of nine scattered 32-byte sectors
@@ -76,7 +75,7 @@ struct StepParams {
   int nx, ny;
   unsigned ns;                 // population plane stride (elements)
   int tiles_per_row, ntiles;   // bulk tiling: one tile = kBlock consecutive cells of a row
-  int nbulk, nlink;            // blocks in each launch
+  int nbulk, nlink;            // bulk tiles and link blocks of a step
   int coll, forced;
   double op, om, gx, gy;
   double sqrt_cs2;
@@ -103,7 +102,7 @@ struct StepParams {
   unsigned nbs;
   // Staged link kernel: one thread per link, nlinkblk blocks of kBlock links; lnode[l] = boundary
   // node (CSR index) of link l. Launch ranges (a step may launch each kernel in two parts): link
-  // blocks [link_b0, link_b0 + link_n) and bulk tiles [bulk_b0, bulk_b0 + bulk_n), clipped.
+  // blocks [link_b0, link_b0 + link_n) and bulk rows [bulk_b0, bulk_b0 + bulk_n), clipped.
   const int32_t* lnode;
   int nlinks, nlinkblk;
   int link_b0, link_n, bulk_b0, bulk_n;
@@ -332,8 +331,8 @@ __global__ void __launch_bounds__(kBlock) k_probe(const __grid_constant__ StepPa
 }
 
 // ------------------------------------------------------------------ bulk kernel
-// Pull + collide for the interior nodes. Block t covers the kBlock consecutive cells of row tile
-// t. The nine population loads are issued together with the flag load, for every cell of the
+// Pull + collide for the interior nodes. Block (t, y) covers the kBlock consecutive cells of tile t
+// of row y. The nine population loads are issued together with the flag load, for every cell of the
 // tile (wrap keeps every neighbour index inside the grid), so no load waits for the flag; only
 // interior cells (flag 0) store. Boundary cells are written by the link kernel, solid cells never.
 template <class S>
@@ -367,9 +366,10 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepPar
                                                  const S* __restrict__ a, S* __restrict__ b) {
   using R = typename Store<S>::R;
   const int nx = p.nx, ny = p.ny;
-  const int tile = (int)blockIdx.x + (STAGED ? p.bulk_b0 : 0);
-  const int y = tile / p.tiles_per_row;
-  const int x = (tile - y * p.tiles_per_row) * kBlock + (int)threadIdx.x;
+  // grid: x = tile of the row, y = row (from p.bulk_b0), so blocks run in row-major tile order
+  const int y = (int)blockIdx.y + p.bulk_b0;
+  const int x = (int)blockIdx.x * kBlock + (int)threadIdx.x;
+  const int tile = y * p.tiles_per_row + (int)blockIdx.x;
   if (!STAGED && x >= nx) return;
   const bool in = x < nx;
   const unsigned idx = (unsigned)(y * nx + x);

@@ -12,14 +12,26 @@ struct LaunchImpl {
   // which: 3 = both kernels of the step, 1 = the link kernel only, 2 = the bulk kernel only
   // (a step launched in two halves, for per-kernel timing). staged: the link-values kernel and the
   // bulk kernel that also updates the boundary cells, which must run in that order.
+  // The bulk kernel over rows [p.bulk_b0, p.bulk_b0 + p.bulk_n) (clipped to the grid), in launches
+  // of at most 65535 rows (the grid's y limit).
+  template <int CK, int STAGED>
+  static void launch_bulk(const StepParams& p, const S* a, S* b, cudaStream_t s) {
+    const int r1 = p.bulk_b0 + p.bulk_n < p.ny ? p.bulk_b0 + p.bulk_n : p.ny;
+    for (int r = p.bulk_b0; r < r1; r += 65535) {
+      StepParams q = p;
+      q.bulk_b0 = r;
+      const int rows = r1 - r < 65535 ? r1 - r : 65535;
+      k_bulk<S, CK, STAGED><<<dim3((unsigned)p.tiles_per_row, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
+    }
+  }
   template <int CK>
   static cudaError_t step_ck(const StepParams& p, const S* a, S* b, cudaStream_t s, int which, bool staged) {
     if (staged) {
       if (which & 1) k_links_stage<S><<<p.nlinkblk - p.link_b0 < p.link_n ? p.nlinkblk - p.link_b0 : p.link_n, kBlock, 0, s>>>(p, a);
-      if (which & 2) k_bulk<S, CK, 1><<<p.nbulk - p.bulk_b0 < p.bulk_n ? p.nbulk - p.bulk_b0 : p.bulk_n, kBlock, 0, s>>>(p, a, b);
+      if (which & 2) launch_bulk<CK, 1>(p, a, b, s);
     } else {
       if (which & 1) k_links<S, CK><<<p.nlink, kBlock, 0, s>>>(p, a, b);
-      if (which & 2) k_bulk<S, CK, 0><<<p.nbulk, kBlock, 0, s>>>(p, a, b);
+      if (which & 2) launch_bulk<CK, 0>(p, a, b, s);
     }
     return cudaGetLastError();
   }
