@@ -54,20 +54,6 @@ VL_HD R wgt(int i) {
   return i == 0 ? Lat<R>::W0 : (i < 5 ? Lat<R>::W1 : Lat<R>::W5);
 }
 
-// 1 / rho of the collision. FP64: the correctly rounded division (the reference's operation).
-// FP32 built with VL_FAST_RECIP: the hardware's approximate divide (__fdividef, within 2 ulp), for
-// the reduced-precision kernels, which are held to a tolerance rather than to bit identity.
-template <class R>
-VL_HD R recip(R rho) {
-  return R(1.0) / rho;
-}
-#if defined(__CUDA_ARCH__) && defined(VL_FAST_RECIP)
-template <>
-__device__ __forceinline__ float recip<float>(float rho) {
-  return __fdividef(1.0f, rho);
-}
-#endif
-
 template <class R>
 VL_HD void equilibrium(R rho, R ux, R uy, R* out) {
   const R usq = R(1.5) * (ux * ux + uy * uy);
@@ -82,7 +68,7 @@ template <class R>
 VL_HD void collide_bgk(R* f, R omega) {
   R rho, jx, jy;
   moments(f, rho, jx, jy);
-  const R inv = recip(rho);
+  const R inv = R(1.0) / rho;
   R feq[9];
   equilibrium(rho, jx * inv, jy * inv, feq);
   R moving = R(0.0);
@@ -99,7 +85,7 @@ template <class R>
 VL_HD void collide_trt(R* f, R op, R om) {
   R rho, jx, jy;
   moments(f, rho, jx, jy);
-  const R inv = recip(rho);
+  const R inv = R(1.0) / rho;
   const R ux = jx * inv, uy = jy * inv;
   const R usq = R(1.5) * (ux * ux + uy * uy);
   R moving = R(0.0);
@@ -124,7 +110,7 @@ template <class R>
 VL_HD void collide_forced(R* f, R op, R om, R gx, R gy) {
   R rho, jx, jy;
   moments(f, rho, jx, jy);
-  const R inv = recip(rho);
+  const R inv = R(1.0) / rho;
   const R ux = jx * inv + R(0.5) * gx, uy = jy * inv + R(0.5) * gy;
   const R fx = rho * gx, fy = rho * gy;
   const R usq = R(1.5) * (ux * ux + uy * uy);
