@@ -214,7 +214,7 @@ def time_to_converged():
             "criterion": "every later 3-period window within 0.5 % of the plain FP64 run on mean c_D and St",
             "plain_converged": s["plain_converged"], "fast_form": arm(s["warm"]), "uniform_start_batched": arm(s["cold"]),
             "seconds": round(time.perf_counter() - t0, 1),
-            "full_study": "200 held-out tunnels: 8.2x median, 5.85x aggregate (profiles/warmstart_study.md)"}
+            "full_study": "200 held-out tunnels: 8.2-8.6x median, 5.85-6.29x aggregate in two runs (profiles/warmstart_study.md)"}
 
 
 def run_vortexlab(args):

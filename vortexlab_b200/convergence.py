@@ -64,13 +64,16 @@ def convergence_step(cd, cl, dt, cd_ref, st_ref, win, tol=0.005):
 
 
 def plain_runs(cases, tol=0.005):
-    """FP64 single-tunnel runs (uniform start), one after the other. Returns per-case dicts with
-    the reference values, steps to convergence and the device milliseconds of the run."""
+    """FP64 single-tunnel runs (uniform start), one after the other, each with the fastest of the
+    step schedules for its grid (timed on its start state before the timed run; every schedule
+    gives the same populations). Returns per-case dicts with the reference values, steps to
+    convergence, the wall time of the run and the schedule used."""
     out = []
     for c in cases:
         tn = c.tunnel
         tn.precision = "f64"
         ch = tn.build(c.body)
+        ch.sim.autotune(4)
         ch.sim.record(c.steps)
         t0 = time.perf_counter()
         ch.step(c.steps)
@@ -82,7 +85,7 @@ def plain_runs(cases, tol=0.005):
         cd_ref, st_ref, win = reference_values(cd, cl, dt)
         conv = convergence_step(cd, cl, dt, cd_ref, st_ref, win, tol)
         out.append(dict(cd_ref=cd_ref, st_ref=st_ref, win=win, conv_steps=conv, steps=c.steps, wall_s=wall,
-                        ms_per_step=1e3 * wall / c.steps, dt=dt, d=tn.d))
+                        ms_per_step=1e3 * wall / c.steps, dt=dt, d=tn.d, schedule=ch.sim.schedule))
         ch.close()
     return out
 
@@ -178,7 +181,7 @@ def warm_comparison(net, cases, refs=None, precision="f32", tol=0.005):
     for k, (c, r) in enumerate(zip(cases, refs)):
         nx, ny = c.tunnel.grid()
         row = dict(kind=c.kind, d=c.params["d"], re=round(c.params["re"], 1), steps=c.steps, cd_ref=r["cd_ref"],
-                   st_ref=r["st_ref"], plain_conv_steps=r["conv_steps"],
+                   st_ref=r["st_ref"], plain_conv_steps=r["conv_steps"], plain_schedule=r["schedule"],
                    plain_s=r["wall_s"] / r["steps"] * r["conv_steps"] if r["conv_steps"] >= 0 else None)
         for name, (res, s_lu, _) in arms.items():
             f = res[k]
@@ -200,8 +203,11 @@ def warm_comparison(net, cases, refs=None, precision="f32", tol=0.005):
                     max_abs_cd_err=float(max(abs(r[f"{name}_cd_err"]) for r in ok)),
                     max_abs_st_err=float(max(abs(r[f"{name}_st_err"]) for r in ok)))
 
+    schedules = {}
+    for r in rows:
+        schedules[r["plain_schedule"]] = schedules.get(r["plain_schedule"], 0) + 1
     summary = dict(tunnels=len(rows), plain_converged=sum(1 for r in rows if r["plain_s"]),
-                   cold=agg("cold"), warm=agg("warm"),
+                   plain_schedules=schedules, cold=agg("cold"), warm=agg("warm"),
                    batch={n: a[2] for n, a in arms.items()})
     return dict(summary=summary, rows=rows)
 
