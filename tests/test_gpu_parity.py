@@ -293,3 +293,23 @@ def test_staged_schedule_follows_every_change_of_state(gpu):
         out.append((sim.state_hash(), sim.force.copy()))
     assert out[0][0] == out[1][0]
     assert _force_close(out[1][1], out[0][1], rel=1e-13)
+
+
+def test_staged_schedule_channel_records_match(gpu):
+    """The 2D-2 rig (parabolic inlet, absorbing outlet, recorded force and pressure drop) through
+    the staged step, split in two parts: the pressure-drop history (evaluated in the step epilogue,
+    from the populations) equals the two-kernel step's bit for bit, the force history to rounding."""
+    V = gpu
+    out = []
+    for sched in ("concurrent", "staged"):
+        r = V.cylinder.rig(V.cylinder.Setup(n=20), 100.0, 1.0)
+        r.ch.sim.schedule = sched
+        out.append(V.cylinder.run_record(r, 700) + (r.ch.sim.state_hash(), r.ch.sim.outlet_density_offset))
+        r.ch.close()
+    (cd0, cl0, dp0, h0, o0), (cd1, cl1, dp1, h1, o1) = out
+    assert h0 == h1 and o0 == o1
+    assert np.array_equal(dp0, dp1)
+    # summation rounding scales with the force's magnitude: the lift, near zero on the symmetric
+    # start, is held to the drag's scale
+    scale = np.max(np.abs(cd0))
+    assert np.max(np.abs(cd1 - cd0)) <= 1e-12 * scale and np.max(np.abs(cl1 - cl0)) <= 1e-12 * scale
