@@ -208,3 +208,25 @@ def test_staged_step_lookup(V, name):
                         assert bfirst[k] <= l < bfirst[k + 1] and dirs[l] == j
                 seen += 1
     assert seen == nb
+
+
+@pytest.mark.parametrize("name", list(_domains().keys()))
+def test_staged_split_point(V, name):
+    """The staged step runs a quarter of its link blocks (256 links each) first, then the bulk
+    tiles of the rows before the row of the node of the first link left to the second part, while
+    that part runs. Replayed on the host tables: every boundary node of those rows has all its links
+    in the first part, and the rows after the split hold every node with a link in the second."""
+    t = S.product_builder(_domains()[name]).link_table()
+    flags, bidx, bfirst = t["flags"], t["bnode_idx"], t["bnode_first"]
+    ny, nx = flags.shape
+    nlinks = int(bfirst[-1])
+    nblk = max(1, (nlinks + 255) // 256)
+    if nblk < 4:
+        pytest.skip("too few links for a split")
+    lnode = np.repeat(np.arange(len(bidx)), np.diff(bfirst))
+    la = nblk // 4
+    first_b = la * 256
+    row = int(bidx[lnode[first_b]]) // nx
+    rows = bidx // nx
+    assert np.all(bfirst[1:][rows < row] <= first_b)
+    assert np.all(rows[lnode[first_b:]] >= row)
