@@ -19,6 +19,7 @@ import os
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -33,6 +34,9 @@ FALLBACK_HBM_GBS = 6650.0
 # profiles/k_bulk_k_links_f64_disk_box.md and profiles/k_links_stage_k_bulk_staged_f64_disk_box.md),
 # per (precision, staged). Scaled to a full launch by nodes.
 NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3, ("f64", True): 140.2}
+NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2048x2048 launch, scaled by nodes"
+# steps of the full-size parity check against the oracle (about 3 s of oracle time on 16 threads)
+PARITY_STEPS = 20
 
 
 def workload_name(prec):
@@ -56,17 +60,26 @@ class ClockSampler:
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
 
+    INTERVAL_MS = 20
+
     def __init__(self, gpu_index):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        fd, self.path = tempfile.mkstemp(prefix="vl_clocks_", suffix=".csv")
+        os.close(fd)
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.INTERVAL_MS)],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+        # wait (at most 5 s) for the first sample, so that the sampling covers what follows
+        t0 = time.perf_counter()
+        while self.proc is not None and time.perf_counter() - t0 < 5.0:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
+                break
+            time.sleep(0.01)
 
     def stop(self):
         if self.proc is None:
@@ -78,7 +91,10 @@ class ClockSampler:
             self.proc.kill()
         self.f.close()
         rows = []
-        for line in open(self.path):
+        with open(self.path) as fh:
+            lines = fh.readlines()
+        os.unlink(self.path)
+        for line in lines:
             p = [x.strip() for x in line.split(",")]
             if len(p) < 8:
                 continue
@@ -92,7 +108,7 @@ class ClockSampler:
         reasons = sorted({names[k] for _, _, r in rows for k in range(4) if r[k].lower() == "active"})
         loaded = [r[0] for r in rows if r[0] > 0.5 * r[1]] or [r[0] for r in rows]
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "interval_ms": self.INTERVAL_MS}
 
 
 def dist_setup(world):
@@ -123,13 +139,34 @@ def dist_sum(dist, v):
     return float(t.item())
 
 
+def _workloads():
+    """The seeded workload generators (vortexlab_b200/workloads.py, numpy only), loaded from their
+    file so that the CPU legs import nothing of the CUDA library."""
+    import importlib.util
+    name = "_vl_workloads_standalone"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "vortexlab_b200", "workloads.py"))
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        sys.modules[name] = mod
+    return sys.modules[name]
+
+
+def box_config(prec, fluid, interior, links, bnodes, world):
+    """The workload's description, identical in both arms."""
+    return {"workload": workload_name(prec), "grid": [BOX["nx"], BOX["ny"]], "fluid_nodes": int(fluid),
+            "interior_nodes": int(interior), "links": int(links), "boundary_nodes": int(bnodes),
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (populations 2 x 9 x 33.5M values), no flush needed"}
+
+
 def oracle_box(threads):
+    """The box on the oracle (the reference's FP64 CPU algorithm restated), at the uniform start."""
     import numpy as np
 
     import oracle as O
-    from vortexlab_b200.workloads import disk_field
     nx, ny = BOX["nx"], BOX["ny"]
-    disks = disk_field(nx, ny, BOX["seed"], BOX["fraction"])
+    disks = _workloads().disk_field(nx, ny, BOX["seed"], BOX["fraction"])
     b = O.Builder(nx, ny)
     b.periodic_x = b.periodic_y = True
     b.tau = BOX["tau"]
@@ -141,10 +178,11 @@ def oracle_box(threads):
     return sim
 
 
-def time_oracle(threads, max_steps, budget_s):
-    """Times the oracle (the reference's CPU algorithm restated, row-split threads as in its pool)
-    on the box: one untimed step, then as many full steps as fit the budget (at most max_steps)."""
-    sim = oracle_box(threads)
+def time_oracle(sim, threads, max_steps, budget_s):
+    """Times the oracle on `threads` host threads (row-split pool, serial link pass, as the
+    reference's pool): one untimed step, then as many full steps as fit the budget (at most
+    max_steps)."""
+    sim.set_threads(threads)
     t0 = time.perf_counter()
     sim.step(1)
     one = time.perf_counter() - t0
@@ -155,18 +193,60 @@ def time_oracle(threads, max_steps, budget_s):
     return sim.fluid_nodes() * steps / secs / 1e6, steps, secs
 
 
+def box_parity(sim, pops, hist, steps, osim):
+    """The full box after `steps` steps from the uniform start on the device (populations `pops`,
+    per-step force `hist`) against the oracle run from the same start: state hash (FNV-1a over
+    every fluid population, src/sim.rs:654-668), largest population difference, and the force of
+    every step relative to the largest oracle force."""
+    import numpy as np
+    t0 = time.perf_counter()
+    fo = np.zeros((steps, 2))
+    for k in range(steps):
+        osim.step(1)
+        fo[k] = osim.force[0]
+    ref = osim.populations().reshape(-1)
+    max_abs = 0.0
+    chunk = 1 << 24
+    for i in range(0, ref.size, chunk):
+        max_abs = max(max_abs, float(np.max(np.abs(ref[i:i + chunk] - pops[i:i + chunk]))))
+    del ref
+    hg, ho = sim.state_hash(), osim.state_hash()
+    fg = hist[:steps, :2]
+    force_rel = float(np.max(np.abs(fg - fo)) / max(np.max(np.abs(fo)), 1e-300))
+    return {"steps": steps, "state_hash_gpu": f"{hg:016x}", "state_hash_oracle": f"{ho:016x}",
+            "hash_equal": hg == ho, "max_abs_pop": max_abs, "force_rel": force_rel,
+            "bars": "populations 1e-10 absolute (bit-identical expected), force 1e-9 relative",
+            "ok": bool(max_abs <= 1e-10 and force_rel <= 1e-9),
+            "seconds": round(time.perf_counter() - t0, 1)}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    import numpy as np
     threads = os.cpu_count() or 1
-    mlups, steps, secs = time_oracle(threads, max(args.steps, 1), budget_s=60.0)
-    sample = f"{steps} full steps of the {BOX['nx']}x{BOX['ny']} box after 1 untimed step ({secs:.1f} s)"
+    sim = oracle_box(threads)
+    flags = sim.flags()
+    interior = int(np.count_nonzero(flags == 0))
+    warm = max(args.warmup, 0)
+    t0 = time.perf_counter()
+    sim.step(max(warm, 1))
+    one = (time.perf_counter() - t0) / max(warm, 1)
+    # every timed step is a full step of the box; at most about two minutes of them
+    steps = int(max(1, min(args.steps, 120.0 / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    sim.step(steps)
+    secs = time.perf_counter() - t0
+    mlups = sim.fluid_nodes() * steps / secs / 1e6
+    sample = f"{steps} full steps of the {BOX['nx']}x{BOX['ny']} box after {max(warm, 1)} untimed ({secs:.1f} s)"
     line = {
         "impl": "reference", "metric": "MLUPS", "value": round(mlups, 2), "unit": "MLUPS", "n_gpus": args.gpus,
-        "steps": steps, "warmup": 1, "ms_per_step": round(1e3 * secs / steps, 3), "higher_is_better": True,
+        "steps": steps, "warmup": max(warm, 1), "ms_per_step": round(1e3 * secs / steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": workload_name("f64"), "threads": threads},
+        "config": box_config("f64", sim.fluid_nodes(), interior, sim.link_count(), sim.bnode_count(), args.gpus),
+        "run": {"threads": threads, "code": "oracle/liboracle.so: the reference's FP64 CPU step restated in C++ "
+                                            "(row-split thread pool, serial link pass)"},
         "cpu_baseline": {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": round(mlups, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -217,6 +297,53 @@ def time_to_converged():
             "full_study": "200 held-out tunnels: 8.2-8.6x median, 5.85-6.29x aggregate in two runs (profiles/warmstart_study.md)"}
 
 
+def bulk_roofline(prec, staged, fluid, interior, steps, link_ms, bulk_ms, total_ms):
+    """Roofline of the dominant kernel, the bulk kernel: pull + collide of the interior nodes, or of
+    every fluid node in the staged step (whose first kernel only evaluates the link rules)."""
+    peak, peak_kind = hbm_peak()
+    bpl = BYTES_PER_LU[prec]
+    bulk_nodes = fluid if staged else interior
+    achieved = bulk_nodes * bpl / (bulk_ms * 1e-3 / steps) / 1e9
+    traffic = NCU_DRAM_BYTES_PER_LU.get((prec, staged))
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+            "traffic": None if traffic is None else round(traffic * bulk_nodes),
+            "traffic_source": None if traffic is None else NCU_TRAFFIC_SOURCE,
+            "kernel": ("k_bulk (staged: all fluid nodes; both launches of a step, with the second link "
+                       "part beside them)") if staged else "k_bulk (interior nodes)",
+            "bytes_per_node_update": bpl,
+            "algorithmic_bytes_per_launch": bulk_nodes * bpl,
+            "kernel_ms_per_launch": round(bulk_ms / steps, 4),
+            "link_kernel_ms_per_launch": round(link_ms / steps, 4),
+            "bulk_share": round(bulk_ms / max(bulk_ms + link_ms, 1e-12), 4),
+            "step_frac_of_peak": round(fluid * bpl / (total_ms * 1e-3 / steps) / 1e9 / peak, 4)}
+
+
+def box_variant(V, prec, steps, warmup):
+    """The same box with populations stored in `prec` (the narrower storage of the fast form):
+    MLUPS and the bulk kernel's roofline, device-timed like the headline."""
+    import numpy as np
+
+    from vortexlab_b200.workloads import build_disk_box, disk_field
+    disks = disk_field(BOX["nx"], BOX["ny"], BOX["seed"], BOX["fraction"])
+    sim = build_disk_box(V, BOX["nx"], BOX["ny"], disks, tau=BOX["tau"], precision=prec)
+    interior = int(np.count_nonzero(sim.flags() == 0))
+    fluid = sim.fluid_nodes()
+    sim.init((1.0, BOX["u"], 0.0))
+    tune = sim.autotune(8)
+    sim.step(max(warmup, 3))
+    sim.synchronize()
+    link_ms, bulk_ms, total_ms = sim.step_profiled(steps)
+    out = {"workload": workload_name(prec), "steps": steps, "schedule": sim.schedule,
+           "autotune_ms_per_step": tune, "mlups": round(fluid * steps / (total_ms * 1e-3) / 1e6, 1),
+           "ms_per_step": round(total_ms / steps, 4),
+           "roofline": bulk_roofline(prec, sim.schedule == "staged", fluid, interior, steps, link_ms, bulk_ms,
+                                     total_ms),
+           "finite": bool(np.isfinite(sim.force).all())}
+    sim.close()
+    return out
+
+
 def run_vortexlab(args):
     import numpy as np
 
@@ -240,53 +367,36 @@ def run_vortexlab(args):
     tune = sim.autotune(8) if args.schedule == "auto" else None
     if args.schedule != "auto":
         sim.schedule = args.schedule
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    gpu_index = vis.split(",")[local] if vis and len(vis.split(",")) > local else local
+    n = nx * ny
+    rho_h, ux_h, uy_h, pops_h = (V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(9 * n))
+    rho_h.array[:] = 1.0
+    ux_h.array[:] = BOX["u"]
+    uy_h.array[:] = 0.0
+    sim.synchronize()
+    # clocks are sampled from the warm-up through the timed region and the end-to-end run
+    sampler = ClockSampler(gpu_index)
     sim.step(max(args.warmup, 3))
     sim.synchronize()
     if dist:
         dist.barrier()
     sim.synchronize()
-    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
-    gpu_index = vis.split(",")[local] if vis and len(vis.split(",")) > local else local
-    sampler = ClockSampler(gpu_index)
     launches0 = sim.launch_count()
     link_ms, bulk_ms, total_ms = sim.step_profiled(args.steps)
     launches = sim.launch_count() - launches0
-    clocks = sampler.stop()
     sim.synchronize()
     if dist:
         dist.barrier()
     total_ms_max = dist_max(dist, total_ms)
     secs = total_ms_max * 1e-3
     value = world * fluid * args.steps / secs / 1e6
-
-    # roofline of the dominant kernel, the bulk kernel: pull + collide of the interior nodes, or of
-    # every fluid node in the staged step (whose first kernel only evaluates the link rules)
-    peak, peak_kind = hbm_peak()
-    bpl = BYTES_PER_LU[prec]
     staged = sim.schedule == "staged"
-    bulk_nodes = fluid if staged else interior
-    bulk_launch_s = bulk_ms * 1e-3 / args.steps
-    achieved = bulk_nodes * bpl / bulk_launch_s / 1e9
-    traffic = NCU_DRAM_BYTES_PER_LU.get((prec, staged))
-    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
-                "traffic": None if traffic is None else round(traffic * bulk_nodes),
-                "kernel": ("k_bulk (staged: all fluid nodes; both launches of a step, with the second link "
-                           "part beside them)") if staged else "k_bulk (interior nodes)",
-                "algorithmic_bytes_per_launch": bulk_nodes * bpl,
-                "kernel_ms_per_launch": round(bulk_ms / args.steps, 4),
-                "link_kernel_ms_per_launch": round(link_ms / args.steps, 4),
-                "bulk_share": round(bulk_ms / max(bulk_ms + link_ms, 1e-12), 4),
-                "step_frac_of_peak": round(fluid * bpl / (total_ms * 1e-3 / args.steps) / 1e9 / peak, 4)}
+    roofline = bulk_roofline(prec, staged, fluid, interior, args.steps, link_ms, bulk_ms, total_ms)
 
     # end to end through the public API with host buffers: upload the start field from pinned host
     # memory, run the steps with the per-step force recorded on the device, download the force
     # history and the final populations.
-    n = nx * ny
-    rho_h, ux_h, uy_h, pops_h = (V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(n), V.PinnedArray(9 * n))
-    rho_h.array[:] = 1.0
-    ux_h.array[:] = BOX["u"]
-    uy_h.array[:] = 0.0
     sim.synchronize()
     if dist:
         dist.barrier()
@@ -297,22 +407,22 @@ def run_vortexlab(args):
     hist = sim.history()
     sim.populations(out=pops_h.array)
     e2e_s = time.perf_counter() - t0
+    clocks = sampler.stop()
     e2e_s = dist_max(dist, e2e_s)
     e2e_value = world * fluid * args.steps / e2e_s / 1e6
     h2d = 3 * n * 8
     d2h = hist.nbytes + 9 * n * 8
     finite = bool(np.isfinite(hist[:, :2]).all())
+    if clocks is not None:
+        clocks["window"] = "warm-up, timed region and end-to-end run"
 
     line = {
         "metric": "MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(total_ms_max / args.steps, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": prec, "data": "synthetic",
-        "config": {"workload": workload_name(prec), "grid": [nx, ny], "fluid_nodes": fluid, "interior_nodes": interior,
-                   "links": sim.link_count(), "boundary_nodes": sim.bnode_count(), "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (populations 2 x 9 x 33.5M values), no flush needed",
-                   "timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
-                   "schedule": sim.schedule, "autotune_ms_per_step": tune,
-                   "setup_s": round(setup_s, 2)},
+        "config": box_config(prec, fluid, interior, sim.link_count(), sim.bnode_count(), world),
+        "run": {"timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
+                "schedule": sim.schedule, "autotune_ms_per_step": tune, "setup_s": round(setup_s, 2)},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(d2h / args.steps), "seconds": round(e2e_s, 4),
@@ -321,19 +431,36 @@ def run_vortexlab(args):
         "gpu_launches": int(dist_sum(dist, launches)),
         "clocks": clocks,
     }
+    osim = None
+    threads = os.cpu_count() or 1
+    if rank == 0 and world == 1 and not args.no_parity and prec == "f64":
+        # the full box against the oracle: PARITY_STEPS steps from the uniform start on both
+        osim = oracle_box(threads)
+        ps = PARITY_STEPS
+        sim.init((1.0, BOX["u"], 0.0))
+        sim.record(ps)
+        sim.step(ps)
+        ph = sim.history()
+        sim.populations(out=pops_h.array)
+        line["parity"] = box_parity(sim, pops_h.array, ph, ps, osim)
+        line["parity"]["schedule"] = sim.schedule
     del rho_h, ux_h, uy_h, pops_h
     sim.close()
     if rank == 0 and world == 1 and not args.no_extras:
+        line["precision_f32"] = box_variant(V, "f32", args.steps, args.warmup)
+        line["precision_f16s"] = box_variant(V, "f16s", args.steps, args.warmup)
         line["channel_n80"] = channel_n80(V)
         line["time_to_converged"] = time_to_converged()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        mlups, steps, secs = time_oracle(threads, 50, budget_s=15.0)
-        m1, s1, t1 = time_oracle(1, 20, budget_s=8.0)
+        if osim is None:
+            osim = oracle_box(threads)
+        mlups, steps, secs = time_oracle(osim, threads, 50, budget_s=15.0)
+        m1, s1, t1 = time_oracle(osim, 1, 20, budget_s=8.0)
         line["cpu_baseline"] = {"value": round(mlups, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
                                 "sample": f"{steps} full steps of the same box after 1 untimed step ({secs:.1f} s)",
                                 "single_thread": {"value": round(m1, 2), "cores": 1,
                                                   "sample": f"{s1} full steps after 1 untimed step ({t1:.1f} s)"}}
+    del osim
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -351,6 +478,7 @@ def main():
     ap.add_argument("--precision", choices=["f64", "f32", "f16s"], default="f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first", "staged"])
     ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
     args = ap.parse_args()

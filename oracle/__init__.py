@@ -83,6 +83,7 @@ def _declare(L):
         "vlo_sim_bnode_count": (sz, [vp]),
         "vlo_sim_pnode_count": (sz, [vp]),
         "vlo_sim_threads": (sz, [vp]),
+        "vlo_sim_set_threads": (None, [vp, sz]),
         "vlo_sim_ngroups": (i, [vp]),
         "vlo_sim_t": (u64, [vp]),
         "vlo_sim_flags": (None, [vp, P(C.c_uint8)]),
@@ -393,6 +394,10 @@ class Sim:
 
     def threads(self):
         return lib().vlo_sim_threads(self.ptr)
+
+    def set_threads(self, threads):
+        """Runs later steps on a pool of ``threads`` workers (results do not depend on it)."""
+        lib().vlo_sim_set_threads(self.ptr, threads)
 
     def flags(self):
         out = np.zeros(self.n, dtype=np.uint8)

@@ -1248,6 +1248,9 @@ size_t vlo_sim_link_count(void* s) { return ((Sim*)s)->links.size(); }
 size_t vlo_sim_bnode_count(void* s) { return ((Sim*)s)->bnodes.size(); }
 size_t vlo_sim_pnode_count(void* s) { return ((Sim*)s)->pnodes.size(); }
 size_t vlo_sim_threads(void* s) { return ((Sim*)s)->pool->threads(); }
+// Replaces the worker pool (the same row split over another thread count; results do not depend
+// on it, tests/solver.rs:270-291).
+void vlo_sim_set_threads(void* s, size_t threads) { ((Sim*)s)->pool = std::make_unique<Pool>(threads); }
 int vlo_sim_ngroups(void* s) { return (int)(((Sim*)s)->force.size() / 2); }
 uint64_t vlo_sim_t(void* s) { return ((Sim*)s)->t; }
 void vlo_sim_flags(void* s, uint8_t* out) {
