@@ -132,6 +132,12 @@ int vl_builder_fill_shape(vl_builder* b, int kind);                        /* :1
  * 1 + (nx + 1) + 3 * ny) values. For testing the host compiler against the oracle. */
 int vl_builder_link_table(vl_builder* b, size_t* nlinks, size_t* nbnodes, size_t* npnodes, uint8_t* flags,
                           int32_t* bnode_idx, int32_t* bnode_first, double* link_f64, int32_t* link_i32);
+/* Host-side view of how the staged step (VL_SCHEDULE_STAGED) splits its work, without touching a
+ * GPU: links per block of its link kernel, link blocks, the blocks run before the first bulk part
+ * (0 = the step is not split) and the rows of that first bulk part. No reference counterpart (the
+ * reference's link pass is serial); for testing the split rule on the tables it is applied to. */
+int vl_builder_stage_split(vl_builder* b, int* links_per_block, int* link_blocks, int* split_blocks,
+                           int* split_rows);
 /* Builder::build + Sim::from_builder (:134-136, :219-354): classifies the cells, builds the
  * boundary-node and link lists once on the host, uploads them and allocates the population
  * buffers in the given storage precision. Consumes `b` (freed on success and on failure). */
@@ -227,7 +233,9 @@ int vl_sim_launch_count(vl_sim* s, uint64_t* out);
  *   out4         device pointer to 4 doubles: mass, momentum x, momentum y, largest speed
  *   stream       cudaStream_t to run on (NULL: the default stream); returns before completion
  * The first call on a device looks up the array's device address (once per device, with that
- * device current); make that first call before any stream capture. Every call reuses the same
+ * device current) and keeps it for the life of the process; make that first call before any
+ * stream capture. A cudaDeviceReset (or any other teardown of the device's primary context)
+ * invalidates that address: do not call this function on that device again in the same process. Every call reuses the same
  * array and overwrites each slot it reads, so nothing needs clearing, but calls whose kernels
  * overlap on the GPU (other streams, other host threads) race on it. */
 #define VL_REDUCE_STATIC_MAX_CELLS 33554432

@@ -212,21 +212,26 @@ def test_staged_step_lookup(V, name):
 
 @pytest.mark.parametrize("name", list(_domains().keys()))
 def test_staged_split_point(V, name):
-    """The staged step runs a quarter of its link blocks (256 links each) first, then the bulk
-    tiles of the rows before the row of the node of the first link left to the second part, while
-    that part runs. Replayed on the host tables: every boundary node of those rows has all its links
-    in the first part, and the rows after the split hold every node with a link in the second."""
-    t = S.product_builder(_domains()[name]).link_table()
+    """The staged step runs a part of its link blocks first, then the bulk tiles of the rows before
+    the row of the node of the first link left to the second part, while that part runs. The split
+    the library computes (vl_builder_stage_split, the same function the device sim uses) is checked
+    on the host tables: every boundary node of those rows has all its links in the first part, and
+    the rows after the split hold every node with a link in the second."""
+    bld = S.product_builder(_domains()[name])
+    sp = bld.stage_split()
+    t = bld.link_table()
     flags, bidx, bfirst = t["flags"], t["bnode_idx"], t["bnode_first"]
     ny, nx = flags.shape
     nlinks = int(bfirst[-1])
-    nblk = max(1, (nlinks + 255) // 256)
-    if nblk < 4:
-        pytest.skip("too few links for a split")
+    per = sp["links_per_block"]
+    assert sp["link_blocks"] == max(1, (nlinks + per - 1) // per)
+    if sp["split_blocks"] == 0:
+        pytest.skip("the step is not split on this domain")
+    assert 0 < sp["split_blocks"] < sp["link_blocks"] and 0 < sp["split_rows"] < ny
     lnode = np.repeat(np.arange(len(bidx)), np.diff(bfirst))
-    la = nblk // 4
-    first_b = la * 256
-    row = int(bidx[lnode[first_b]]) // nx
+    first_b = sp["split_blocks"] * per
+    row = sp["split_rows"]
+    assert int(bidx[lnode[first_b]]) // nx == row
     rows = bidx // nx
     assert np.all(bfirst[1:][rows < row] <= first_b)
     assert np.all(rows[lnode[first_b:]] >= row)

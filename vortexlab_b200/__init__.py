@@ -412,6 +412,14 @@ class Builder:
         return dict(flags=flags.reshape(self.ny, self.nx), bnode_idx=bidx, bnode_first=bfirst,
                     link_f64=lf.reshape(-1, 5), link_i32=li.reshape(-1, 7), npnodes=npn.value)
 
+    def stage_split(self):
+        """How the staged step splits its work on these tables (host only): dict with
+        links_per_block, link_blocks, split_blocks (0: not split) and split_rows."""
+        self._apply()
+        v = [C.c_int() for _ in range(4)]
+        check(lib.vl_builder_stage_split(self._h, *(C.byref(x) for x in v)))
+        return dict(zip(("links_per_block", "link_blocks", "split_blocks", "split_rows"), (x.value for x in v)))
+
     def build(self, threads: Optional[int] = None, precision="f64") -> "Sim":
         """Builder::build (src/sim.rs:134-136). ``threads`` is accepted for API compatibility: the
         reference's thread pool (src/pool.rs) is replaced by one CUDA stream."""

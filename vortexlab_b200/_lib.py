@@ -78,6 +78,7 @@ def _declare(L):
         "vl_builder_add_radiating": (i, [vp, d]),
         "vl_builder_fill_rect": (i, [vp, sz, sz, sz, sz, i]),
         "vl_builder_fill_shape": (i, [vp, i]),
+        "vl_builder_stage_split": (i, [vp, P(i), P(i), P(i), P(i)]),
         "vl_builder_link_table": (i, [vp, P(sz), P(sz), P(sz), P(C.c_uint8), P(C.c_int32), P(C.c_int32), P(d),
                                       P(C.c_int32)]),
         "vl_builder_build": (vp, [vp, i]),

@@ -482,6 +482,23 @@ bool staged_tables(const vl::CompiledDomain& d, int tiles_per_row, std::vector<i
 #endif
 
 // Creates the device-resident sim for a compiled domain.
+// Split point of the staged step: a fraction 1 / VL_STAGE_SPLIT of the link blocks, and the row
+// tiles before the row of the node of the first link they leave to the second part (every
+// boundary node of the earlier rows has all its links in the first part). 0, 0: one part.
+void staged_split(const vl::CompiledDomain& d, const std::vector<int32_t>& lnode, int& split_links, int& split_rows) {
+  split_links = split_rows = 0;
+  const int per = vl::kBlock * vl::kStagePer;
+  const int nlinkblk = std::max(1, ((int)d.links.size() + per - 1) / per);
+  if (nlinkblk >= VL_STAGE_SPLIT) {
+    const int la = nlinkblk / VL_STAGE_SPLIT;
+    const int row = d.bnode_idx[(size_t)lnode[(size_t)la * per]] / (int)d.nx;
+    if (row > 0) {
+      split_links = la;
+      split_rows = row;
+    }
+  }
+}
+
 vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -605,17 +622,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
   P.bulk_n = P.ny;
-  // Split point of the staged step: a fraction 1 / VL_STAGE_SPLIT of the link blocks, and the row
-  // tiles before the row of the node of the first link they leave to the second part (every
-  // boundary node of the earlier rows has all its links in the first part).
-  if (P.nlinkblk >= VL_STAGE_SPLIT) {
-    const int la = P.nlinkblk / VL_STAGE_SPLIT;
-    const int row = d.bnode_idx[(size_t)lnode[(size_t)la * vl::kBlock * vl::kStagePer]] / (int)d.nx;
-    if (row > 0) {
-      s->split_links = la;
-      s->split_rows = row;
-    }
-  }
+  staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;
   P.lb = s->d_lb;
@@ -854,6 +861,25 @@ int vl_builder_link_table(vl_builder* b, size_t* nlinks, size_t* nbnodes, size_t
       o[5] = L.behind; o[6] = ((L.flags >> 2) & 3) - 1 + 3 * (((L.flags >> 4) & 3) - 1 + 1) + 1;
     }
   }
+  return VL_OK;
+}
+
+int vl_builder_stage_split(vl_builder* b, int* links_per_block, int* link_blocks, int* split_blocks,
+                           int* split_rows) {
+  if (!b) return fail(VL_EINVAL, "null builder");
+  vl::CompiledDomain dom;
+  std::string err;
+  if (!vl::compile_domain(b->spec, dom, err)) return fail(VL_EINVAL, err);
+  std::vector<int32_t> lnode(dom.links.size());
+  for (size_t k = 0; k + 1 < dom.bnode_first.size(); ++k)
+    for (int l = dom.bnode_first[k]; l < dom.bnode_first[k + 1]; ++l) lnode[(size_t)l] = (int32_t)k;
+  const int per = vl::kBlock * vl::kStagePer;
+  int sl = 0, sr = 0;
+  staged_split(dom, lnode, sl, sr);
+  if (links_per_block) *links_per_block = per;
+  if (link_blocks) *link_blocks = std::max(1, ((int)dom.links.size() + per - 1) / per);
+  if (split_blocks) *split_blocks = sl;
+  if (split_rows) *split_rows = sr;
   return VL_OK;
 }
 

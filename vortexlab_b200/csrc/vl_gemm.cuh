@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
   __shared__ __align__(8) uint64_t full[STAGES], empty[STAGES], done;
   __shared__ uint32_t tmem_base;
   __shared__ int failed;
+  __shared__ int issued_loads;   // k-blocks whose TMA loads the producer issued
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
@@ -162,6 +163,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
     }
     mbar_init(&done, 1);
     failed = 0;
+    issued_loads = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -200,11 +202,7 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
       }
       issued = kb + 1;
     }
-    if (failed) {
-      // Drain: wait (bounded) for the copies still in flight before the block can exit.
-      for (int kb = issued > stages ? issued - stages : 0; kb < issued; ++kb)
-        mbar_wait(&full[kb % stages], (uint32_t)(kb / stages) & 1u, ep.spin_limit);
-    }
+    issued_loads = issued;
   } else if (threadIdx.x == 32) {
     // MMA issuer.
     const uint32_t idesc = instr_desc_bf16(BN, op);
@@ -242,9 +240,17 @@ __global__ void __launch_bounds__(128, 1) k_gemm_bf16(const __grid_constant__ CU
   // (lane = row). Each 32 x 32 block goes through shared memory (the idle stage buffers) so that
   // the global stores are row-contiguous across the warp: lane = column.
   const bool have = mbar_wait(&done, 0, ep.spin_limit);
+  if (!have) atomicExch(&failed, 1);
   asm volatile("tcgen05.fence::after_thread_sync;");
-  __syncwarp();
-  const bool good = have && !failed;
+  __syncthreads();   // the producer has finished issuing; every thread sees the same `failed`
+  const bool good = !failed;
+  if (!good && threadIdx.x == 0) {
+    // Drain: whichever thread gave up, wait (bounded) for the TMA copies that may still be landing
+    // in this CTA's shared memory (the last `stages` issued loads) before the block can exit.
+    const int issued = issued_loads;
+    for (int kb = issued > stages ? issued - stages : 0; kb < issued; ++kb)
+      mbar_wait(&full[kb % stages], (uint32_t)(kb / stages) & 1u, ep.spin_limit);
+  }
   if (good) {
     // the stage buffers were last read by the tensor cores (async proxy): order those reads before
     // this warp's generic writes to the same memory

@@ -699,15 +699,38 @@ def compare(n_test=200, eval_units=100.0, log=print):
     return dict(config=dict(n_test=n_test, eval_units=eval_units, network=PRETRAINED), comparison=out)
 
 
+def profile_training(steps=6, fields=48, batch=16, seed=1):
+    """Trains the full network for `steps` Adam steps on `fields` seeded random fields (synthetic
+    inputs, targets and masks of the training shapes): the command the training-step profiles are
+    taken on. Returns milliseconds per step over the timed run of `train` (after a first run that
+    loads the kernels; device synchronised on both sides)."""
+    torch = _t()
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal((fields, H, W, CIN)).astype(np.float32)
+    y = rng.standard_normal((fields, H, W, NT)).astype(np.float32)
+    w = (rng.random((fields, H, W)) > 0.05).astype(np.float32)
+    data = Dataset(x, y, w)
+    net = UNet()
+    train(net, data, epochs=1, batch=batch)                     # first step: set-up and module loading
+    per_epoch = fields // batch
+    log = train(net, data, epochs=max(1, -(-steps // per_epoch)), batch=batch)
+    return 1e3 * log.seconds / max(log.steps, 1)
+
+
 if __name__ == "__main__":
     # python -m vortexlab_b200.warmstart OUTDIR [n_train n_test gen_units eval_units train_seconds epochs]
     # python -m vortexlab_b200.warmstart compare OUTDIR [n_test eval_units]   (the shipped network)
+    # python -m vortexlab_b200.warmstart profile [steps]   (training steps on random fields)
     import json
     import sys
 
     def log(m):
         print(m, flush=True)
 
+    if sys.argv[1] == "profile":
+        n = int(sys.argv[2]) if len(sys.argv) > 2 else 6
+        print(json.dumps({"training_ms_per_step": round(profile_training(n), 3), "steps": n}), flush=True)
+        sys.exit(0)
     if sys.argv[1] == "compare":
         outdir = sys.argv[2]
         os.makedirs(outdir, exist_ok=True)
