@@ -210,6 +210,12 @@ enum { VL_SCHEDULE_CONCURRENT = 0, VL_SCHEDULE_LINKS_FIRST = 1, VL_SCHEDULE_BULK
        VL_SCHEDULE_COUNT = 4 };
 int vl_sim_set_schedule(vl_sim* s, int schedule);
 int vl_sim_get_schedule(const vl_sim* s);
+/* FP32 and 16-bit storage: how many neighbouring cells of a row one thread of the bulk kernel
+ * updates. 2 (the default) moves every population plane as one vector per thread and runs the
+ * collision on packed FP32 pairs, where the row length is even and no body force is set (else one
+ * cell per thread); 1 forces one cell per thread. Results are bit-identical either way. No
+ * reference counterpart (the reference updates one cell per loop iteration, src/sim.rs:700-735). */
+int vl_sim_set_cells_per_thread(vl_sim* s, int cells);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the
  * fastest. ms (may be NULL) receives the milliseconds per step of the VL_SCHEDULE_COUNT
@@ -285,6 +291,9 @@ int vl_batch_size(const vl_batch* b);
 int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_t* fluid_nodes, uint64_t* steps);
 /* Bulk tile shape: 2^log2_tx cells x ty rows = 256 cells (32 <= 2^log2_tx <= 256). */
 int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty);
+/* FP32 and 16-bit storage: 2 (the default where every tunnel's row length is even) bulk cells of a
+ * row per thread, as vl_sim_set_cells_per_thread, or 1. Results are bit-identical either way. */
+int vl_batch_set_cells_per_thread(vl_batch* b, int cells);
 int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty);
 int vl_batch_set_schedule(vl_batch* b, int schedule);  /* VL_SCHEDULE_* */
 /* Times the tile shapes 256x1, 128x2, 64x4, 32x8 on the current state without advancing it and
@@ -300,6 +309,9 @@ int vl_batch_launch_count(const vl_batch* b, uint64_t* out);
 int vl_batch_status(vl_batch* b, int k, uint64_t* t, int* nonfinite, double* force2);
 /* Force (fx, fy) of tunnel k after each of its steps so far: 2 * count doubles. */
 int vl_batch_force_history(vl_batch* b, int k, double* out, uint64_t* count);
+/* The records of steps [first, first + max) of tunnel k that exist so far (count receives how
+ * many; 2 doubles each): the increments an on-line stopping rule reads between runs. */
+int vl_batch_force_history_range(vl_batch* b, int k, uint64_t first, uint64_t max, double* out, uint64_t* count);
 /* FP64 populations of tunnel k (reference layout, 9 * nx * ny values), its flags, its state hash. */
 int vl_batch_download(vl_batch* b, int k, double* out);
 /* Ends tunnel k after `steps` steps instead of the count it was added with (which stays the upper

@@ -1,7 +1,6 @@
 """Batched tunnels: a tunnel advanced in a batch with others of other sizes, shapes and Reynolds
-numbers matches the same tunnel run alone (state and per-step force), in every tile shape and
-kernel schedule (bit-identical in FP64; the FP32 kernels may fuse multiply-adds differently from
-the single-tunnel ones); autotuning does not perturb the run."""
+numbers matches the same tunnel run alone (state and per-step force) bit for bit, in every tile
+shape, kernel schedule and storage format; autotuning does not perturb the run."""
 import numpy as np
 import pytest
 
@@ -14,8 +13,12 @@ def _cases(V):
     return cases
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16s"])
 def test_batched_tunnels_match_single_runs(gpu, prec):
+    """Every tile shape and schedule, and for the narrow formats both bulk forms (two cells per
+    thread, one): the batched tunnel's populations and force history are bit-identical to the
+    tunnel run alone (FP64: the reference's operation order; FP32 / 16-bit: the explicit FP32
+    operators that every narrow kernel shares)."""
     V = gpu
     from vortexlab_b200.batch import Batch
     cases = _cases(V)
@@ -27,37 +30,25 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
         ch.step(c.steps)
         single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.populations().copy()))
         ch.close()
-    first = {}
-    for tile, sched in [("256x1", "concurrent"), ("64x4", "links-first"), ("32x8", "bulk-first"),
-                        ("128x2", "staged"), ("32x8", "staged")]:
+    runs = [("256x1", "concurrent", 2), ("64x4", "links-first", 2), ("32x8", "bulk-first", 2),
+            ("128x2", "staged", 2), ("32x8", "staged", 2)]
+    if prec != "f64":
+        runs += [("256x1", "concurrent", 1), ("128x2", "staged", 1)]
+    for tile, sched, cells in runs:
         b = Batch(prec)
         for c in cases:
             b.add(c.tunnel.spec(c.body), c.steps)
         b.build()
         b.tile = tile
         b.schedule = sched
+        b.set_cells_per_thread(cells)
         b.run()
-        hashes = []
         for k, c in enumerate(cases):
             t, nonfinite, _ = b.status(k)
             assert t == c.steps and not nonfinite
-            hashes.append(b.state_hash(k))
-            if prec == "f64":
-                assert hashes[-1] == single[k][0], (tile, sched, k)
-                assert np.array_equal(b.force_history(k), single[k][1]), (tile, sched, k)
-            else:
-                # FP32 rounding: 1e-6 for the kernels shared with the single-tunnel step; the staged
-                # pair collides boundary cells in the bulk kernel, whose multiply-add contraction
-                # rounds differently, and the flow amplifies those last-bit differences to ~2e-6
-                tol, ftol = (1e-5, 1e-3) if sched == "staged" else (1e-6, 1e-4)
-                assert np.max(np.abs(b.populations(k) - single[k][2])) <= tol, (tile, sched, k)
-                h = b.force_history(k)
-                assert np.max(np.abs(h - single[k][1])) <= ftol * np.max(np.abs(single[k][1])), (tile, sched, k)
-        # every tile shape and schedule: bit-identical (FP32 / FP16: the staged pair collides the
-        # boundary cells in the bulk kernel, whose multiply-add contraction may differ in the last bit)
-        group = "all" if prec == "f64" else sched == "staged"
-        first.setdefault(group, hashes)
-        assert hashes == first[group], (tile, sched)
+            assert b.state_hash(k) == single[k][0], (tile, sched, cells, k)
+            assert np.array_equal(b.populations(k), single[k][2]), (tile, sched, cells, k)
+            assert np.array_equal(b.force_history(k), single[k][1]), (tile, sched, cells, k)
         b.close()
 
 

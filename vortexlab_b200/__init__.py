@@ -651,6 +651,10 @@ class Sim:
     def schedule(self, name: str):
         check(lib.vl_sim_set_schedule(self._h, self.SCHEDULES[name]))
 
+    def set_cells_per_thread(self, cells: int):
+        """FP32 / 16-bit storage: 2 (default) bulk cells per thread where possible, or 1."""
+        check(lib.vl_sim_set_cells_per_thread(self._h, cells))
+
     def autotune(self, steps_each: int = 8):
         """Times the four kernel schedules without advancing the state; keeps the fastest.
         Returns {schedule: ms per step}."""

@@ -111,6 +111,7 @@ def _declare(L):
         "vl_sim_set_dp_probe": (i, [vp, d, d, d, d]),
         "vl_sim_last_step_ms": (i, [vp, P(f)]),
         "vl_sim_step_profiled": (i, [vp, u64, P(d), P(d), P(d)]),
+        "vl_sim_set_cells_per_thread": (i, [vp, i]),
         "vl_sim_set_schedule": (i, [vp, i]),
         "vl_sim_get_schedule": (i, [vp]),
         "vl_sim_autotune": (i, [vp, i, P(d)]),
@@ -129,6 +130,7 @@ def _declare(L):
         "vl_batch_build": (i, [vp]),
         "vl_batch_size": (i, [vp]),
         "vl_batch_tunnel_info": (i, [vp, i, P(sz), P(sz), P(sz), P(u64)]),
+        "vl_batch_set_cells_per_thread": (i, [vp, i]),
         "vl_batch_set_tile": (i, [vp, i, i]),
         "vl_batch_get_tile": (i, [vp, P(i), P(i)]),
         "vl_batch_set_schedule": (i, [vp, i]),
@@ -138,6 +140,7 @@ def _declare(L):
         "vl_batch_global_step": (i, [vp, P(u64)]),
         "vl_batch_launch_count": (i, [vp, P(u64)]),
         "vl_batch_status": (i, [vp, i, P(u64), P(i), P(d)]),
+        "vl_batch_force_history_range": (i, [vp, i, u64, u64, P(d), P(u64)]),
         "vl_batch_force_history": (i, [vp, i, P(d), P(u64)]),
         "vl_batch_download": (i, [vp, i, P(d)]),
         "vl_batch_init": (i, [vp, i, P(d), P(d), P(d)]),

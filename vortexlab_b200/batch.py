@@ -88,6 +88,10 @@ class Batch:
     def schedule(self, name):
         check(lib.vl_batch_set_schedule(self._h, self.SCHEDULES[name]))
 
+    def set_cells_per_thread(self, cells: int):
+        """FP32 / 16-bit storage: 2 (default where every row length is even) bulk cells per thread, or 1."""
+        check(lib.vl_batch_set_cells_per_thread(self._h, cells))
+
     def autotune(self, steps_each=4):
         """Times the four tile shapes without advancing the tunnels; keeps the fastest."""
         out = np.zeros(4)
@@ -122,6 +126,13 @@ class Batch:
         check(lib.vl_batch_force_history(self._h, k, None, C.byref(cnt)))
         out = np.zeros(2 * max(cnt.value, 1))
         check(lib.vl_batch_force_history(self._h, k, _dp(out), C.byref(cnt)))
+        return out[: 2 * cnt.value].reshape(cnt.value, 2)
+
+    def force_history_range(self, k, first: int, max_count: int) -> np.ndarray:
+        """Force records of steps [first, first + max_count) that tunnel k has run so far."""
+        cnt = C.c_uint64()
+        out = np.zeros(2 * max(int(max_count), 1))
+        check(lib.vl_batch_force_history_range(self._h, k, int(first), int(max_count), _dp(out), C.byref(cnt)))
         return out[: 2 * cnt.value].reshape(cnt.value, 2)
 
     def populations(self, k) -> np.ndarray:

@@ -204,6 +204,17 @@ struct vl_sim {
     return cudaSuccess;
   }
 
+  int set_cells_per_thread(int c) {
+    if (c != 1 && c != 2) return fail(VL_EINVAL, "cells per thread must be 1 or 2");
+    if ((c == 2) != (P.pairs != 0) && gexec) {
+      VL_CUDA(cudaStreamSynchronize(stream));
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    P.pairs = c == 2 ? 1 : 0;
+    return VL_OK;
+  }
+
   int set_schedule(int sc) {
     if (sc < 0 || sc >= VL_SCHEDULE_COUNT) return fail(VL_EINVAL, "schedule must be 0, 1, 2 or 3");
     if (sc != schedule && gexec) {
@@ -622,6 +633,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
   P.bulk_n = P.ny;
+  P.pairs = 1;
   staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;
@@ -1272,6 +1284,11 @@ int vl_sim_set_schedule(vl_sim* s, int schedule) {
 }
 
 int vl_sim_get_schedule(const vl_sim* s) { return s ? s->schedule : VL_EINVAL; }
+
+int vl_sim_set_cells_per_thread(vl_sim* s, int cells) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  return s->set_cells_per_thread(cells);
+}
 
 int vl_sim_autotune(vl_sim* s, int steps_each, double* ms3) {
   if (!s || steps_each < 1) return fail(VL_EINVAL, "autotune: bad arguments");

@@ -51,6 +51,7 @@ int upload(T** dst, const std::vector<T>& v) {
 struct vl_batch {
   int device = 0;
   int prec = VL_F32;
+  bool pairs_ok = false;   // narrow storage and every tunnel's row length even
   const vl::Launchers* L = nullptr;
   std::vector<vl::ChannelPlan> plans;
   std::vector<uint64_t> steps;
@@ -112,7 +113,7 @@ struct vl_batch {
   int build_lists(bool all) {
     tiles_h.clear();
     chunks_h.clear();
-    const int tx = 1 << log2_tx;
+    const int tx = (1 << log2_tx) << (P.pairs ? 1 : 0);   // cells per tile row
     for (size_t k = 0; k < tun.size(); ++k) {
       if (!all && s >= tun[k].steps) continue;
       const vl::BatchTunnel& T = tun[k];
@@ -469,6 +470,13 @@ int vl_batch_build(vl_batch* b) {
   P.lb = b->d_lb;
   P.ownc = b->d_ownc;
   P.nbs = nbs;
+  P.pairs = 0;
+  if (!precision_is_f64(b->prec)) {
+    bool even = true;
+    for (const auto& T : b->tun) even = even && T.nx % 2 == 0 && T.ns % 2 == 0;
+    P.pairs = even ? 1 : 0;
+  }
+  b->pairs_ok = P.pairs != 0;
   b->built = true;
   // The host plans (domains) are no longer needed on the host except their sizes.
   for (auto& pl : b->plans) {
@@ -495,6 +503,15 @@ int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty) {
     return fail(VL_EINVAL, "tile must be 2^log2_tx x ty = 256 cells with 32 <= 2^log2_tx <= 256");
   b->log2_tx = log2_tx;
   b->ty = ty;
+  return b->build_lists(false);
+}
+
+int vl_batch_set_cells_per_thread(vl_batch* b, int cells) {
+  if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
+  if (cells != 1 && cells != 2) return fail(VL_EINVAL, "cells per thread must be 1 or 2");
+  const int want = cells == 2 && b->pairs_ok ? 1 : 0;
+  if (want == b->P.pairs) return VL_OK;
+  b->P.pairs = want;
   return b->build_lists(false);
 }
 
@@ -569,6 +586,20 @@ int vl_batch_force_history(vl_batch* b, int k, double* out, uint64_t* count) {
   if (out && have)
     VB_CUDA(cudaMemcpy(out, b->d_hist + 2 * b->tun[k].hist_off, have * 2 * sizeof(double), cudaMemcpyDeviceToHost));
   *count = have;
+  return VL_OK;
+}
+
+int vl_batch_force_history_range(vl_batch* b, int k, uint64_t first, uint64_t max, double* out, uint64_t* count) {
+  if (!b || !b->built || !count || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  vl::BatchState st;
+  int rc = pull_state(b, k, &st);
+  if (rc) return rc;
+  const uint64_t have = std::min<uint64_t>(st.t, b->tun[k].steps);
+  const uint64_t n = first >= have ? 0 : std::min<uint64_t>(have - first, max);
+  if (out && n)
+    VB_CUDA(cudaMemcpy(out, b->d_hist + 2 * (b->tun[k].hist_off + first), n * 2 * sizeof(double),
+                       cudaMemcpyDeviceToHost));
+  *count = n;
   return VL_OK;
 }
 

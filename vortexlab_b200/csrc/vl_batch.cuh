@@ -21,6 +21,7 @@
 #pragma once
 
 #include "vl_device.cuh"
+#include "vl_pair.cuh"
 
 namespace vl {
 
@@ -78,6 +79,9 @@ struct BatchParams {
   void* lb;
   void* ownc;
   unsigned nbs;
+  // narrow storage with every row length even: the bulk kernel is the two-cell form and a tile is
+  // 2 * 2^log2_tx cells wide
+  int pairs;
 };
 
 // Controls of a tunnel at its step t (src/cases/channel.rs:118-130).
@@ -132,10 +136,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
       }
     }
   }
-  if (T.coll == COLL_BGK)
-    collide_bgk(f, (R)T.op);
-  else
-    collide_trt(f, (R)T.op, (R)T.om);
+  collide_s<S>(f, T.coll == COLL_BGK ? 0 : 1, (R)T.op, (R)T.om, R(0), R(0));
   if (fl > (STAGED ? 1 : 0)) return;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * T.ns + idx, i, f[i]);
@@ -144,6 +145,34 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
 #pragma unroll
     for (int i = 0; i < 9; ++i) Store<S>::st(oc + (unsigned)i * p.nbs + (unsigned)g, i, f[i]);
   }
+}
+
+// The two-cell form of k_batch_bulk for narrow storage (every tunnel's row length even): a tile is
+// 2 * 2^log2_tx cells x ty rows, thread t of the tile updates the pair at 2 (t mod 2^log2_tx) of
+// row t / 2^log2_tx; a warp covers 64 cells of one row (2^log2_tx >= 32).
+template <class S, int STAGED>
+__global__ void __launch_bounds__(kBlock) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
+                                                        S* __restrict__ B) {
+  const int4 td = __ldg(p.tiles + blockIdx.x);
+  const BatchTunnel& T = p.tun[td.x];
+  PairTask t;
+  t.nx = T.nx;
+  t.ny = T.ny;
+  t.y = td.y + (int)(threadIdx.x >> p.log2_tx);
+  t.xw = td.z + 2 * (int)((threadIdx.x & ((1u << p.log2_tx) - 1u)) & ~31u);
+  if (t.y >= t.ny || t.xw >= t.nx) return;   // uniform over the warp
+  t.ns = T.ns;
+  t.flag = p.flag + T.cell_off;
+  t.ck = T.coll == COLL_BGK ? 0 : 1;
+  t.op = (float)T.op;
+  t.om = (float)T.om;
+  t.wfirst = STAGED ? __ldg(p.seg_bfirst + T.seg_off + t.y * T.segs + (t.xw >> 5)) : 0;
+  t.kend = T.b_off + T.nb;
+  t.bdesc = p.bdesc;
+  t.lb = (const float*)p.lb;
+  t.ownc = p.ownc;
+  t.nbs = p.nbs;
+  pair_update<S, STAGED>(t, A + T.pop_off, B + T.pop_off);
 }
 
 // STAGED = 1: the link rules only (k_links_stage for a chunk): own populations from the compact

@@ -36,6 +36,7 @@
 #include <cstdint>
 
 #include "vl_lattice.hpp"
+#include "vl_narrow.cuh"
 
 namespace vl {
 
@@ -106,6 +107,9 @@ struct StepParams {
   const int32_t* lnode;
   int nlinks, nlinkblk;
   int link_b0, link_n, bulk_b0, bulk_n;
+  // narrow storage: 1 = the bulk kernel updates two cells of a row per thread where it can
+  // (even row length, no body force), 0 = one cell per thread
+  int pairs;
 };
 
 struct alignas(16) LinkRecDev {
@@ -152,6 +156,32 @@ struct Store<__half> {
 };
 
 // ------------------------------------------------------------------ helpers
+// The collision of storage S: the reference's operators in its operation order for FP64
+// (vl_lattice.hpp), the FP32 operators with explicit multiply-adds for the narrow formats
+// (vl_narrow.cuh; the forced collision keeps the generic form). ck: 0 BGK, 1 TRT, 2 forced.
+template <class S>
+__device__ __forceinline__ void collide_s(typename Store<S>::R* f, int ck, typename Store<S>::R op,
+                                          typename Store<S>::R om, typename Store<S>::R gx, typename Store<S>::R gy) {
+  if (ck == 2)
+    collide_forced(f, op, om, gx, gy);
+  else if (ck == 0)
+    collide_bgk(f, op);
+  else
+    collide_trt(f, op, om);
+}
+template <>
+__device__ __forceinline__ void collide_s<float>(float* f, int ck, float op, float om, float gx, float gy) {
+  if (ck == 2)
+    collide_forced(f, op, om, gx, gy);
+  else if (ck == 0)
+    collide_bgk_n(f, op);
+  else
+    collide_trt_n(f, op, om);
+}
+template <>
+__device__ __forceinline__ void collide_s<__half>(float* f, int ck, float op, float om, float gx, float gy) {
+  collide_s<float>(f, ck, op, om, gx, gy);
+}
 template <class R>
 __device__ __forceinline__ R pick(const R* f, int i) {
   R v = f[0];
@@ -393,13 +423,7 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepPar
       }
     }
   }
-  const R op = (R)p.op, om = (R)p.om, gx = (R)p.gx, gy = (R)p.gy;
-  if (CK == 2)
-    collide_forced(f, op, om, gx, gy);
-  else if (CK == 0)
-    collide_bgk(f, op);
-  else
-    collide_trt(f, op, om);
+  collide_s<S>(f, CK, (R)p.op, (R)p.om, (R)p.gx, (R)p.gy);
   if (fl > (STAGED ? 1 : 0)) return;
 #pragma unroll
   for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * p.ns + idx, i, f[i]);
@@ -582,12 +606,7 @@ __device__ __forceinline__ void link_node(const S* __restrict__ a, unsigned ns, 
   for (int d = 0; d < 9; ++d) own[d] = Store<S>::ld(a + (unsigned)d * ns + idx, d);
   link_rules<S>(a, ns, own, first, last, links, vs, drho, gx_, gy_, sqrt_cs2, acc,
                 [&](int, int i, R back) { set_dir(f, i, back); });
-  if (ck == 2)
-    collide_forced(f, op, om, gx, gy);
-  else if (ck == 0)
-    collide_bgk(f, op);
-  else
-    collide_trt(f, op, om);
+  collide_s<S>(f, ck, op, om, gx, gy);
 }
 
 // Block partial of the first `ncomp` force components: fixed shuffle tree within each warp, then

@@ -1,9 +1,12 @@
 // Launcher bodies shared by the per-precision translation units.
 #pragma once
 
+#include <type_traits>
+
 #include "vl_batch.cuh"
 #include "vl_device.cuh"
 #include "vl_launch.hpp"
+#include "vl_pair.cuh"
 
 namespace vl {
 
@@ -14,6 +17,16 @@ struct LaunchImpl {
   // bulk kernel that also updates the boundary cells, which must run in that order.
   // The bulk kernel over rows [p.bulk_b0, p.bulk_b0 + p.bulk_n) (clipped to the grid), in launches
   // of at most 65535 rows (the grid's y limit).
+  // Narrow storage with rows of even length and no body force: the two-cell kernel (k_bulk2, one
+  // block per 2 * kBlock cells of a row); otherwise the one-cell kernel (one block per kBlock).
+  template <int CK>
+  static bool use_pairs(const StepParams& p) {
+    if constexpr (std::is_same<S, double>::value || CK == 2) {
+      return false;
+    } else {
+      return p.pairs && p.nx % 2 == 0 && p.ns % 2 == 0;
+    }
+  }
   template <int CK, int STAGED>
   static void launch_bulk(const StepParams& p, const S* a, S* b, cudaStream_t s) {
     const int r1 = p.bulk_b0 + p.bulk_n < p.ny ? p.bulk_b0 + p.bulk_n : p.ny;
@@ -21,6 +34,13 @@ struct LaunchImpl {
       StepParams q = p;
       q.bulk_b0 = r;
       const int rows = r1 - r < 65535 ? r1 - r : 65535;
+      if constexpr (!std::is_same<S, double>::value && CK != 2) {
+        if (use_pairs<CK>(p)) {
+          const unsigned tiles = (unsigned)((p.nx + 2 * kBlock - 1) / (2 * kBlock));
+          k_bulk2<S, CK, STAGED><<<dim3(tiles, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
+          continue;
+        }
+      }
       k_bulk<S, CK, STAGED><<<dim3((unsigned)p.tiles_per_row, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
     }
   }
@@ -89,12 +109,24 @@ struct LaunchImpl {
   // which: 1 link kernel, 2 bulk kernel, 3 both; + 4 the staged pair.
   static cudaError_t batch_step(const BatchParams& p, int ntiles, int nchunks, int which, const void* a, void* b,
                                 cudaStream_t s) {
+    bool pairs = false;
+    if constexpr (!std::is_same<S, double>::value) pairs = p.pairs != 0;
     if (which & 4) {
       if ((which & 1) && nchunks > 0) k_batch_links<S, 1><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
-      if ((which & 2) && ntiles > 0) k_batch_bulk<S, 1><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      if ((which & 2) && ntiles > 0) {
+        if constexpr (!std::is_same<S, double>::value) {
+          if (pairs) k_batch_bulk2<S, 1><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+        }
+        if (!pairs) k_batch_bulk<S, 1><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      }
     } else {
       if ((which & 1) && nchunks > 0) k_batch_links<S, 0><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
-      if ((which & 2) && ntiles > 0) k_batch_bulk<S, 0><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      if ((which & 2) && ntiles > 0) {
+        if constexpr (!std::is_same<S, double>::value) {
+          if (pairs) k_batch_bulk2<S, 0><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+        }
+        if (!pairs) k_batch_bulk<S, 0><<<ntiles, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
+      }
     }
     return cudaGetLastError();
   }

@@ -689,12 +689,16 @@ def study(n_train=2000, n_test=200, gen_units=50.0, eval_units=100.0, train_seco
 
 
 def compare(n_test=200, eval_units=100.0, log=print):
-    """The time-to-converged comparison of `study` with the shipped network (no training)."""
-    from . import convergence as CV
+    """The time-to-converged comparison with the shipped network (no training): every run stops
+    on-line from its own history, warm-start failures fall back to the uniform start, every tunnel
+    is counted (online.comparison)."""
+    from . import online as OL
     from .batch import seeded_tunnels
     test = seeded_tunnels(seed=TEST_SEED, count=n_test, units=eval_units)
+    net = load_pretrained()
+    predict(net, np.zeros((1, H, W, CIN), np.float32))     # resident network, kernels loaded
     t0 = time.perf_counter()
-    out = CV.warm_comparison(load_pretrained(), test)
+    out = OL.comparison(test, net, max_units=eval_units, log=log)
     log(f"comparison in {time.perf_counter() - t0:.1f} s: {out['summary']}")
     return dict(config=dict(n_test=n_test, eval_units=eval_units, network=PRETRAINED), comparison=out)
 
