@@ -58,6 +58,7 @@ def _declare(L):
         "vlo_shape_rotated": (vp, [vp, d, d, d]),
         "vlo_shape_translated": (vp, [vp, d, d]),
         "vlo_shape_outside_band": (vp, [d, d]),
+        "vlo_shape_star": (vp, [d, d, P(d), i, d]),
         "vlo_shape_ellipse": (vp, [d, d, d, d]),
         "vlo_shape_section": (vp, [i, d, d, d, d, d]),
         "vlo_shape_bitmap": (vp, [sz, sz, P(C.c_float), d, d, d]),
@@ -242,6 +243,11 @@ class Shape:
     @staticmethod
     def outside_band(y0, y1):
         return Shape(lib().vlo_shape_outside_band(y0, y1))
+
+    @staticmethod
+    def star(cx, cy, radii, phase):
+        r = _arr(radii)
+        return Shape(lib().vlo_shape_star(cx, cy, _dp(r), len(r), phase))
 
     @staticmethod
     def ellipse(cx, cy, a, b):

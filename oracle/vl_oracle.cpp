@@ -1158,6 +1158,17 @@ void* vlo_shape_translated(void* inner, double dx, double dy) {
 void* vlo_shape_outside_band(double y0, double y1) {
   auto s = new OutsideBand(); s->y0 = y0; s->y1 = y1; return (Shape*)s;
 }
+// The star-convex polygon of the batched-tunnel workload (no counterpart in the reference's
+// shapes): vertex k at angle phase + 2 pi k / n, distance radii[k] from (cx, cy).
+void* vlo_shape_star(double cx, double cy, const double* radii, int n, double phase) {
+  auto s = new Polygon();
+  for (int k = 0; k < n; ++k) {
+    const double th = phase + 2.0 * M_PI * (double)k / (double)n;
+    s->px.push_back(cx + radii[k] * std::cos(th));
+    s->py.push_back(cy + radii[k] * std::sin(th));
+  }
+  return (Shape*)s;
+}
 void* vlo_shape_ellipse(double cx, double cy, double a, double b) {
   auto s = new Ellipse(); s->cx = cx; s->cy = cy; s->a = a; s->b = b; return (Shape*)s;
 }

@@ -175,3 +175,32 @@ def poiseuille(rows=16, tau=0.8, q=0.8, collision=("trt", 3.0 / 16.0)):
     return dict(nx=nx, ny=ny, periodic=(True, False), tau=tau, collision=collision, accel=(g, 0.0),
                 kinds=[("wall", None, 0, 0, shape)],
                 paint=[("rect", 0, nx - 1, 0, 0, 1), ("rect", 0, nx - 1, ny - 1, ny - 1, 1)])
+
+
+def oracle_shape(body):
+    """The oracle's copy of a product shape description (the batched-tunnel bodies)."""
+    import vortexlab_b200 as V
+    if isinstance(body, V.Rotated):
+        return O.Shape.rotated(oracle_shape(body.inner), body.cx, body.cy, body.angle)
+    if isinstance(body, V.Translated):
+        return O.Shape.translated(oracle_shape(body.inner), body.dx, body.dy)
+    if isinstance(body, V.Ellipse):
+        return O.Shape.ellipse(body.cx, body.cy, body.a, body.b)
+    if isinstance(body, V.Star):
+        return O.Shape.star(body.cx, body.cy, list(body.radii), body.phase)
+    if isinstance(body, V.Polygon):
+        return O.Shape.polygon(body.pts)
+    if isinstance(body, V.Circle):
+        return O.Shape.circle(body.cx, body.cy, body.r)
+    raise TypeError(f"no oracle shape for {type(body).__name__}")
+
+
+def oracle_channel(spec, threads=1):
+    """The oracle's Channel (src/cases/channel.rs:71-116) for a product Spec."""
+    kick = None
+    if spec.kick is not None:
+        k = spec.kick
+        kick = (k.cx, k.cy, k.omega, float(k.start), float(k.duration))
+    coll = O.BGK if spec.collision.kind == 0 else O.TRT
+    return O.Channel(spec.nx, spec.ny, spec.inflow[0], spec.inflow[1], spec.nu, coll, oracle_shape(spec.body),
+                     spec.ramp_steps, kick, threads, spec.collision.magic)

@@ -8,7 +8,22 @@ import scenarios as S
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16s"])
+def c16_stored(v32, w32):
+    """The value the custom 16-bit format (sign, 3-bit exponent, 12-bit mantissa of f_i - w_i) stores
+    for FP32 populations v32 of weight w32, restated on the host: (v - w) 2^-118 rounded once to FP32,
+    its bit pattern rounded to 12 mantissa bits (ties to even) and clamped, then decoded and w added
+    back in one rounding."""
+    y = ((v32.astype(np.float64) - w32.astype(np.float64)) * 2.0 ** -118).astype(np.float32)
+    b = y.view(np.uint32).astype(np.uint64)
+    mag = np.minimum(b & 0x7FFFFFFF, 0x03FFF800)
+    r = (mag + 0x3FF + ((mag >> 11) & 1)) >> 11
+    code = r | ((b >> 16) & 0x8000)
+    bits = (((code & 0x7FFF) << 11) | ((code & 0x8000) << 16)).astype(np.uint32)
+    x = bits.view(np.float32).astype(np.float64) * 2.0 ** 118
+    return (x + w32.astype(np.float64)).astype(np.float32)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c"])
 def test_storage_round_trip(gpu, prec):
     """Sim::init writes equilibria; the download returns them rounded to the storage format."""
     V = gpu
@@ -23,6 +38,9 @@ def test_storage_round_trip(gpu, prec):
     fe = ref.populations()
     if prec == "f32":
         expect = fe.astype(np.float32).astype(np.float64)
+    elif prec == "f16c":
+        w32 = np.broadcast_to(w[:, None, None].astype(np.float32), fe.shape)
+        expect = c16_stored(fe.astype(np.float32), w32).astype(np.float64)
     else:
         expect = (w[:, None, None].astype(np.float32)
                   + (fe.astype(np.float32) - w[:, None, None].astype(np.float32)).astype(np.float16).astype(np.float32)
@@ -43,7 +61,7 @@ def test_f32_schafer_turek_2d2_matches_f64(gpu):
         assert abs(vb - va) <= tol * abs(va), (k, va, vb)
 
 
-@pytest.mark.parametrize("prec,tol", [("f32", 1e-6), ("f16s", 5e-4)])
+@pytest.mark.parametrize("prec,tol", [("f32", 1e-6), ("f16s", 5e-4), ("f16c", 5e-4)])
 def test_decaying_swirl_matches_f64(gpu, prec, tol):
     """Periodic box, TRT, 400 steps of a decaying swirl: velocity and density fields against FP64."""
     d = S.periodic_box(48, 36, 0.62, ("trt", 3.0 / 16.0))

@@ -138,6 +138,8 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
   }
   collide_s<S>(f, T.coll == COLL_BGK ? 0 : 1, (R)T.op, (R)T.om, R(0), R(0));
   if (fl > (STAGED ? 1 : 0)) return;
+  if (Saturates<S>::value && !density_plausible(f))
+    mark_diverged(&p.st[td.x].nonfinite, &p.st[td.x].nonfinite_t, &p.st[td.x].t);
 #pragma unroll
   for (int i = 0; i < 9; ++i) Store<S>::st(b + (unsigned)i * T.ns + idx, i, f[i]);
   if (STAGED && fl == 1 && g < T.b_off + T.nb) {
@@ -172,6 +174,9 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk2(const __grid_constant__ 
   t.lb = (const float*)p.lb;
   t.ownc = p.ownc;
   t.nbs = p.nbs;
+  t.bad = &p.st[td.x].nonfinite;
+  t.bad_t = &p.st[td.x].nonfinite_t;
+  t.t_now = &p.st[td.x].t;
   pair_update<S, STAGED>(t, A + T.pop_off, B + T.pop_off);
 }
 

@@ -48,5 +48,6 @@ int set_error(int code, const char* msg);
 const Launchers& launchers_f64();
 const Launchers& launchers_f32();
 const Launchers& launchers_f16s();
+const Launchers& launchers_f16c();
 
 }  // namespace vl

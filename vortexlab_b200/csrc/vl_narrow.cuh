@@ -89,9 +89,9 @@ __device__ __forceinline__ void cu_n(const NMacro<V>& m, V* cu) {
 }
 
 // BGK (src/lattice.rs:80-95): f_i -= omega (f_i - feq_i); the rest population relaxes towards
-// rho - sum of the moving equilibria.
+// rho - sum of the moving equilibria. Returns rho.
 template <class V>
-__device__ __forceinline__ void collide_bgk_n(V* f, float omega) {
+__device__ __forceinline__ V collide_bgk_n(V* f, float omega) {
   using O = NOps<V>;
   const NMacro<V> m = macro_n(f);
   V cu[4];
@@ -112,12 +112,13 @@ __device__ __forceinline__ void collide_bgk_n(V* f, float omega) {
     moving = O::add(moving, O::add(ea, eb));
   }
   f[0] = O::fma(nom, O::sub(f[0], O::sub(m.rho, moving)), f[0]);
+  return m.rho;
 }
 
 // TRT on the pairs (1,3), (2,4), (5,7), (6,8) (src/lattice.rs:100-119): the symmetric part relaxes
-// at op, the antisymmetric part at om; the rest population as in BGK at op.
+// at op, the antisymmetric part at om; the rest population as in BGK at op. Returns rho.
 template <class V>
-__device__ __forceinline__ void collide_trt_n(V* f, float op_, float om_) {
+__device__ __forceinline__ V collide_trt_n(V* f, float op_, float om_) {
   using O = NOps<V>;
   const NMacro<V> m = macro_n(f);
   V cu[4];
@@ -139,6 +140,7 @@ __device__ __forceinline__ void collide_trt_n(V* f, float op_, float om_) {
     moving = O::fma(O::s(2.0f), eq, moving);
   }
   f[0] = O::fma(O::s(-op_), O::sub(f[0], O::sub(m.rho, moving)), f[0]);
+  return m.rho;
 }
 
 }  // namespace vl

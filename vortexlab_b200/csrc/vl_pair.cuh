@@ -55,29 +55,34 @@ struct PairIO<float> {
   static __device__ __forceinline__ Word enc(int, float2 f) { return f; }
 };
 
-// IEEE half of f_i - w_i (the shifted form): a pair is one __half2.
-template <>
-struct PairIO<__half> {
+// The word moves of the 16-bit formats: a pair is one 32-bit word, the first cell in the low half.
+template <class S>
+struct PairIO16 {
   using Word = unsigned;
   using Elem = unsigned;   // the 16-bit value in the low half
-  static __device__ __forceinline__ Word ld(const __half* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
-  static __device__ __forceinline__ Elem ld1(const __half* p) {
+  static __device__ __forceinline__ Word ld(const S* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+  static __device__ __forceinline__ Elem ld1(const S* p) {
     return (unsigned)__ldg(reinterpret_cast<const unsigned short*>(p));
   }
-  static __device__ __forceinline__ void st(__half* p, Word w) { *reinterpret_cast<unsigned*>(p) = w; }
+  static __device__ __forceinline__ void st(S* p, Word w) { *reinterpret_cast<unsigned*>(p) = w; }
   // the low half of the result is the previous lane's high half (or the value at `ep`), the high
   // half the thread's low half
-  static __device__ __forceinline__ Word left(Word v, bool edge, const __half* ep) {
+  static __device__ __forceinline__ Word left(Word v, bool edge, const S* ep) {
     unsigned up = __shfl_up_sync(0xffffffffu, v, 1);
     if (edge) up = ld1(ep) << 16;
     return __byte_perm(up, v, 0x5432);
   }
   // the low half is the thread's high half, the high half the next lane's low half (or `ep`)
-  static __device__ __forceinline__ Word right(Word v, bool edge, const __half* ep) {
+  static __device__ __forceinline__ Word right(Word v, bool edge, const S* ep) {
     unsigned dn = __shfl_down_sync(0xffffffffu, v, 1);
     if (edge) dn = ld1(ep);
     return __byte_perm(v, dn, 0x5432);
   }
+};
+
+// IEEE half of f_i - w_i (the shifted form): a pair is one __half2.
+template <>
+struct PairIO<__half> : PairIO16<__half> {
   static __device__ __forceinline__ float2 dec(int i, Word w) {
     __half2 h;
     *reinterpret_cast<unsigned*>(&h) = w;
@@ -89,6 +94,24 @@ struct PairIO<__half> {
     const float wi = wgt<float>(i);
     const __half2 h = __float22half2_rn(__fadd2_rn(f, make_float2(-wi, -wi)));
     return *reinterpret_cast<const unsigned*>(&h);
+  }
+};
+
+// The custom 16-bit format (c16, vl_device.cuh): the two codes of a word decode to FP32 bit
+// patterns scaled by 2^-118, and one packed fused multiply-add scales them back and adds w_i; the
+// encoding is the packed fused multiply-add that subtracts w_i and scales, then the rounding of each
+// FP32 bit pattern to a 16-bit code.
+template <>
+struct PairIO<c16> : PairIO16<c16> {
+  static __device__ __forceinline__ float2 dec(int i, Word w) {
+    const float2 x = make_float2(__uint_as_float(c16f::lo_bits(w)), __uint_as_float(c16f::hi_bits(w)));
+    const float wi = wgt<float>(i);
+    return __ffma2_rn(x, make_float2(c16f::kUp, c16f::kUp), make_float2(wi, wi));
+  }
+  static __device__ __forceinline__ Word enc(int i, float2 f) {
+    const float sw = -wgt<float>(i) * c16f::kDown;
+    const float2 y = __ffma2_rn(f, make_float2(c16f::kDown, c16f::kDown), make_float2(sw, sw));
+    return c16f::code(__float_as_uint(y.x)) | (c16f::code(__float_as_uint(y.y)) << 16);
   }
 };
 
@@ -120,6 +143,10 @@ struct PairTask {
   const float* lb;
   void* ownc;
   unsigned nbs;
+  // saturating formats: the run's divergence flag, the step it records, and the current step
+  int* bad;
+  unsigned long long* bad_t;
+  const unsigned long long* t_now;
 };
 
 template <class S, int STAGED>
@@ -172,12 +199,13 @@ __device__ __forceinline__ void pair_update(const PairTask& t, const S* __restri
     }
   }
   if (!in) return;
-  if (t.ck == 0)
-    collide_bgk_n(f, t.op);
-  else
-    collide_trt_n(f, t.op, t.om);
+  const float2 rho = t.ck == 0 ? collide_bgk_n(f, t.op) : collide_trt_n(f, t.op, t.om);
   const unsigned idx = rc + (unsigned)x0;
   const bool s0 = fl0 <= STAGED, s1 = fl1 <= STAGED;
+  if (Saturates<S>::value) {
+    const bool ok0 = fabsf(rho.x - 1.0f) < 0.5f, ok1 = fabsf(rho.y - 1.0f) < 0.5f;
+    if ((s0 && !ok0) || (s1 && !ok1)) mark_diverged(t.bad, t.bad_t, t.t_now);
+  }
   if (s0 && s1) {
 #pragma unroll
     for (int i = 0; i < 9; ++i) IO::st(b + (unsigned)i * ns + idx, IO::enc(i, f[i]));
@@ -202,8 +230,11 @@ __device__ __forceinline__ void pair_update(const PairTask& t, const S* __restri
 }
 
 // One sim: block (t, y) updates the 2 * kBlock cells of tile t of row y (from p.bulk_b0).
+#ifndef VL_PAIR_MIN_BLOCKS
+#define VL_PAIR_MIN_BLOCKS 5
+#endif
 template <class S, int CK, int STAGED>
-__global__ void __launch_bounds__(kBlock) k_bulk2(const __grid_constant__ StepParams p, const S* __restrict__ a,
+__global__ void __launch_bounds__(kBlock, VL_PAIR_MIN_BLOCKS) k_bulk2(const __grid_constant__ StepParams p, const S* __restrict__ a,
                                                   S* __restrict__ b) {
   PairTask t;
   t.nx = p.nx;
@@ -222,6 +253,9 @@ __global__ void __launch_bounds__(kBlock) k_bulk2(const __grid_constant__ StepPa
   t.lb = (const float*)p.lb;
   t.ownc = p.ownc;
   t.nbs = p.nbs;
+  t.bad = &p.ctl->nonfinite;
+  t.bad_t = &p.ctl->nonfinite_t;
+  t.t_now = &p.ctl->t;
   pair_update<S, STAGED>(t, a, b);
 }
 

@@ -1,8 +1,10 @@
-// Reduced-precision step kernels: FP32 storage and FP16 storage of f_i - w_i, both with FP32
-// collision arithmetic; the force accumulation and every reduction stay in FP64.
+// Reduced-precision step kernels: FP32 storage, IEEE FP16 storage of f_i - w_i and the custom
+// 16-bit storage of f_i - w_i (c16), all with FP32 collision arithmetic; the force accumulation and
+// every reduction stay in FP64.
 #include "vl_launch_impl.cuh"
 
 namespace vl {
 const Launchers& launchers_f32() { return LaunchImpl<float>::table(); }
 const Launchers& launchers_f16s() { return LaunchImpl<__half>::table(); }
+const Launchers& launchers_f16c() { return LaunchImpl<c16>::table(); }
 }  // namespace vl

@@ -22,7 +22,7 @@ import numpy as np
 from . import cylinder, section, signal
 from .tunnel import Tunnel
 
-PRECISIONS = ("f64", "f32", "f16s")
+PRECISIONS = ("f64", "f32", "f16s", "f16c")
 
 
 def cylinder_2d2(n=80, units=100.0, window=20.0, precisions=PRECISIONS):
