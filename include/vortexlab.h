@@ -213,11 +213,12 @@ enum { VL_SCHEDULE_CONCURRENT = 0, VL_SCHEDULE_LINKS_FIRST = 1, VL_SCHEDULE_BULK
        VL_SCHEDULE_COUNT = 4 };
 int vl_sim_set_schedule(vl_sim* s, int schedule);
 int vl_sim_get_schedule(const vl_sim* s);
-/* FP32 and 16-bit storage: how many neighbouring cells of a row one thread of the bulk kernel
- * updates. 2 (the default) moves every population plane as one vector per thread and runs the
- * collision on packed FP32 pairs, where the row length is even and no body force is set (else one
- * cell per thread); 1 forces one cell per thread. Results are bit-identical either way. No
- * reference counterpart (the reference updates one cell per loop iteration, src/sim.rs:700-735). */
+/* FP32 and 16-bit storage: the most neighbouring cells of a row one thread of the bulk kernel
+ * updates (1, 2 or 4; default 4). With 2 or 4 every population plane moves as one vector per
+ * thread and the collision runs on packed FP32 pairs; the kernel uses the largest of 4, 2, 1 that
+ * is allowed and divides the row length (one cell per thread with a body force). Results are
+ * bit-identical whatever the setting. No reference counterpart (the reference updates one cell
+ * per loop iteration, src/sim.rs:700-735). */
 int vl_sim_set_cells_per_thread(vl_sim* s, int cells);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the

@@ -1,12 +1,12 @@
-"""The two-cell bulk kernel of the narrow storage formats (FP32, 16-bit) against the one-cell kernel.
+"""The multi-cell bulk kernels of the narrow storage formats (FP32, 16-bit) against the one-cell kernel.
 
-With FP32 or 16-bit storage the bulk kernel updates two neighbouring cells per thread where the row
-length is even: vector loads and stores of each population plane, the x-shifted planes completed
-by a warp shuffle (and a memory read at the warp's edges and the periodic wrap), the collision on
-packed FP32 pairs. Every lane performs the one-cell kernel's operations, so the two forms must give
-bit-identical populations, on every link rule and on grids whose rows end inside a warp, in the
-two-kernel and the staged step. The link kernel collides boundary nodes with the same operators, so
-the schedules agree with each other bit for bit as well.
+With FP32 or 16-bit storage the bulk kernel updates 4 or 2 neighbouring cells per thread where the
+row length allows: vector loads and stores of each population plane, the x-shifted planes
+completed by a warp shuffle (and a memory read at the warp's edges and the periodic wrap), the
+collision on packed FP32 pairs. Every lane performs the one-cell kernel's operations, so all forms
+must give bit-identical populations, on every link rule and on grids whose rows end inside a warp,
+in the two-kernel and the staged step. The link kernel collides boundary nodes with the same
+operators, so the schedules agree with each other bit for bit as well.
 """
 import numpy as np
 import pytest
@@ -19,8 +19,11 @@ pytestmark = pytest.mark.gpu
 def _domains():
     from vortexlab_b200.workloads import disk_field
     return {
-        # 640 cells per row: one full 512-cell tile and one whose last four warps are past the row end
+        # 640 cells per row: with 2 cells per thread one full 512-cell tile and one whose last four
+        # warps are past the row end; with 4, one 1024-cell tile of which three warps are
         "disk_box_640x200": S.disk_box(640, 200, disk_field(640, 200, seed=11)),
+        # 1000 cells per row: the last warp of 4-cell groups ends inside the row
+        "disk_box_1000x96": S.disk_box(1000, 96, disk_field(1000, 96, seed=12)),
         # 122 cells per row (a row ends inside a warp), TRT, inlet, absorbing outlet, moving body
         "tunnel_like": S.tunnel_like(radiating=True),
         "tunnel_walls": S.tunnel_like(radiating=False),
@@ -49,14 +52,14 @@ def _run(d, prec, schedule, cells, steps):
     return sim.populations(), sim.history()
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16s"])
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c"])
 @pytest.mark.parametrize("name", list(_domains().keys()))
 def test_two_cell_kernel_matches_one_cell_kernel(gpu, prec, name):
     d = _domains()[name]
     steps = 150
     out = {}
     for schedule in ("concurrent", "staged"):
-        for cells in (2, 1):
+        for cells in (4, 2, 1):
             out[(schedule, cells)] = _run(d, prec, schedule, cells, steps)
     ref_f, ref_h = out[("concurrent", 1)]
     assert np.isfinite(ref_f).all()

@@ -652,7 +652,7 @@ class Sim:
         check(lib.vl_sim_set_schedule(self._h, self.SCHEDULES[name]))
 
     def set_cells_per_thread(self, cells: int):
-        """FP32 / 16-bit storage: 2 (default) bulk cells per thread where possible, or 1."""
+        """FP32 / 16-bit storage: the most bulk cells per thread (1, 2 or 4; default 4)."""
         check(lib.vl_sim_set_cells_per_thread(self._h, cells))
 
     def autotune(self, steps_each: int = 8):

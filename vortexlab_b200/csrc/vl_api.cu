@@ -205,13 +205,13 @@ struct vl_sim {
   }
 
   int set_cells_per_thread(int c) {
-    if (c != 1 && c != 2) return fail(VL_EINVAL, "cells per thread must be 1 or 2");
-    if ((c == 2) != (P.pairs != 0) && gexec) {
+    if (c != 1 && c != 2 && c != 4) return fail(VL_EINVAL, "cells per thread must be 1, 2 or 4");
+    if (c != P.pairs && gexec) {
       VL_CUDA(cudaStreamSynchronize(stream));
       cudaGraphExecDestroy(gexec);
       gexec = nullptr;
     }
-    P.pairs = c == 2 ? 1 : 0;
+    P.pairs = c;
     return VL_OK;
   }
 
@@ -634,7 +634,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
   P.bulk_n = P.ny;
-  P.pairs = 1;
+  P.pairs = 4;
   staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;

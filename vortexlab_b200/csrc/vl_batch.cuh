@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk2(const __grid_constant__ 
   t.bad = &p.st[td.x].nonfinite;
   t.bad_t = &p.st[td.x].nonfinite_t;
   t.t_now = &p.st[td.x].t;
-  pair_update<S, STAGED>(t, A + T.pop_off, B + T.pop_off);
+  group_update<S, 2, STAGED>(t, A + T.pop_off, B + T.pop_off);
 }
 
 // STAGED = 1: the link rules only (k_links_stage for a chunk): own populations from the compact

@@ -107,8 +107,8 @@ struct StepParams {
   const int32_t* lnode;
   int nlinks, nlinkblk;
   int link_b0, link_n, bulk_b0, bulk_n;
-  // narrow storage: 1 = the bulk kernel updates two cells of a row per thread where it can
-  // (even row length, no body force), 0 = one cell per thread
+  // narrow storage: the most cells of a row the bulk kernel's threads update (1, 2 or 4; fewer
+  // where the row length is not a multiple, one with a body force)
   int pairs;
 };
 

@@ -17,27 +17,34 @@ struct LaunchImpl {
   // bulk kernel that also updates the boundary cells, which must run in that order.
   // The bulk kernel over rows [p.bulk_b0, p.bulk_b0 + p.bulk_n) (clipped to the grid), in launches
   // of at most 65535 rows (the grid's y limit).
-  // Narrow storage with rows of even length and no body force: the two-cell kernel (k_bulk2, one
-  // block per 2 * kBlock cells of a row); otherwise the one-cell kernel (one block per kBlock).
+  // Narrow storage without a body force: the multi-cell kernel (k_bulkv, V cells of a row per
+  // thread, one block per V * kBlock cells) with the largest V <= p.pairs that divides the row
+  // length; otherwise the one-cell kernel (one block per kBlock cells).
   template <int CK>
-  static bool use_pairs(const StepParams& p) {
+  static int group_width(const StepParams& p) {
     if constexpr (std::is_same<S, double>::value || CK == 2) {
-      return false;
+      return 1;
     } else {
-      return p.pairs && p.nx % 2 == 0 && p.ns % 2 == 0;
+      if (p.pairs >= 4 && p.nx % 4 == 0 && p.ns % 4 == 0) return 4;
+      if (p.pairs >= 2 && p.nx % 2 == 0 && p.ns % 2 == 0) return 2;
+      return 1;
     }
   }
   template <int CK, int STAGED>
   static void launch_bulk(const StepParams& p, const S* a, S* b, cudaStream_t s) {
     const int r1 = p.bulk_b0 + p.bulk_n < p.ny ? p.bulk_b0 + p.bulk_n : p.ny;
+    const int v = group_width<CK>(p);
     for (int r = p.bulk_b0; r < r1; r += 65535) {
       StepParams q = p;
       q.bulk_b0 = r;
       const int rows = r1 - r < 65535 ? r1 - r : 65535;
       if constexpr (!std::is_same<S, double>::value && CK != 2) {
-        if (use_pairs<CK>(p)) {
-          const unsigned tiles = (unsigned)((p.nx + 2 * kBlock - 1) / (2 * kBlock));
-          k_bulk2<S, CK, STAGED><<<dim3(tiles, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
+        if (v > 1) {
+          const unsigned tiles = (unsigned)((p.nx + v * kBlock - 1) / (v * kBlock));
+          if (v == 4)
+            k_bulkv<S, 4, CK, STAGED><<<dim3(tiles, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
+          else
+            k_bulkv<S, 2, CK, STAGED><<<dim3(tiles, (unsigned)rows), kBlock, 0, s>>>(q, a, b);
           continue;
         }
       }
