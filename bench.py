@@ -368,7 +368,7 @@ def run_vortexlab(args):
     interior = int(np.count_nonzero(flags == 0))
     fluid = sim.fluid_nodes()
     sim.init((1.0, BOX["u"], 0.0))
-    if prec != "f64":
+    if prec != "f64" and args.cells:
         sim.set_cells_per_thread(args.cells)
     tune = sim.autotune(8) if args.schedule == "auto" else None
     if args.schedule != "auto":
@@ -429,7 +429,7 @@ def run_vortexlab(args):
         "config": box_config(prec, fluid, interior, sim.link_count(), sim.bnode_count(), world),
         "run": {"timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
                 "schedule": sim.schedule, "autotune_ms_per_step": tune, "setup_s": round(setup_s, 2),
-                "cells_per_thread": args.cells if prec != "f64" else 1},
+                "cells_per_thread": (args.cells or "default") if prec != "f64" else 1},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(d2h / args.steps), "seconds": round(e2e_s, 4),
@@ -488,8 +488,9 @@ def main():
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first", "staged"])
     ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
-    ap.add_argument("--cells", type=int, default=4, choices=[1, 2, 4],
-                    help="narrow storage: the most bulk cells per thread (Sim.set_cells_per_thread)")
+    ap.add_argument("--cells", type=int, default=0, choices=[0, 1, 2, 4],
+                    help="narrow storage: the most bulk cells per thread (Sim.set_cells_per_thread; 0: the "
+                         "library's default)")
     args = ap.parse_args()
     if args.box:
         nx, ny = (int(v) for v in args.box.lower().split("x"))

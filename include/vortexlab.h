@@ -214,7 +214,7 @@ enum { VL_SCHEDULE_CONCURRENT = 0, VL_SCHEDULE_LINKS_FIRST = 1, VL_SCHEDULE_BULK
 int vl_sim_set_schedule(vl_sim* s, int schedule);
 int vl_sim_get_schedule(const vl_sim* s);
 /* FP32 and 16-bit storage: the most neighbouring cells of a row one thread of the bulk kernel
- * updates (1, 2 or 4; default 4). With 2 or 4 every population plane moves as one vector per
+ * updates (1, 2 or 4; default 2 for FP32, 4 for the 16-bit formats). With 2 or 4 every population plane moves as one vector per
  * thread and the collision runs on packed FP32 pairs; the kernel uses the largest of 4, 2, 1 that
  * is allowed and divides the row length (one cell per thread with a body force). Results are
  * bit-identical whatever the setting. No reference counterpart (the reference updates one cell

@@ -55,3 +55,23 @@ def test_non_finite_history_never_stops():
     cd, cl, dt = _history()
     cd[-10:] = np.nan
     assert settled(cd, cl, dt, StopRule()) is None
+
+
+def test_cached_window_stops_like_the_full_rule():
+    """Reusing the spectral window length between checks (as the on-line batch driver does) stops
+    within one check of the rule evaluated from scratch, with the same settled values to 0.1 %."""
+    cd, cl, dt = _history(units=80.0, settle=25.0)
+    rule = StopRule()
+    t_full, r_full = _first_stop(cd, cl, dt, rule)
+    every = int(2.0 / dt)
+    cache = {}
+    t_cached = r_cached = None
+    for end in range(every, len(cd) + 1, every):
+        r = settled(cd[:end], cl[:end], dt, rule, cache)
+        if r is not None:
+            t_cached, r_cached = end * dt, r
+            break
+    assert t_full is not None and t_cached is not None
+    assert abs(t_cached - t_full) <= 2.0 + 1e-9
+    assert abs(r_cached[0] - r_full[0]) <= 1e-3 * abs(r_full[0])
+    assert abs(r_cached[1] - r_full[1]) <= 1e-3 * r_full[1]

@@ -652,7 +652,8 @@ class Sim:
         check(lib.vl_sim_set_schedule(self._h, self.SCHEDULES[name]))
 
     def set_cells_per_thread(self, cells: int):
-        """FP32 / 16-bit storage: the most bulk cells per thread (1, 2 or 4; default 4)."""
+        """FP32 / 16-bit storage: the most bulk cells per thread (1, 2 or 4; default 2 for FP32, 4
+        for the 16-bit formats)."""
         check(lib.vl_sim_set_cells_per_thread(self._h, cells))
 
     def autotune(self, steps_each: int = 8):

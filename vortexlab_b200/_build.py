@@ -1,9 +1,12 @@
 """Build recipe for libvortexlab_b200.so (in-tree, sm_100a only).
 
 Compiles the host C++ with g++ and the CUDA translation units with nvcc for
-``-gencode arch=compute_100a,code=sm_100a``. The FP64 step kernels are compiled with
-``-fmad=false`` and the host code with ``-ffp-contract=off``: no multiply-add is fused, which keeps
-the FP64 path bit-identical to the reference solver. Run ``python vortexlab_b200/_build.py``.
+``-gencode arch=compute_100a,code=sm_100a``. The step kernels of every storage format are compiled
+with ``-fmad=false`` and the host code with ``-ffp-contract=off``: the compiler fuses no
+multiply-add, which keeps the FP64 path bit-identical to the reference solver and makes every
+narrow-format kernel round exactly as written (their collision spells its fused multiply-adds out
+with intrinsics), so that no two kernels round the same expression differently. Run
+``python vortexlab_b200/_build.py``.
 """
 from __future__ import annotations
 
@@ -46,7 +49,7 @@ def _sources(defines=()):
         ("vl_host.o", [cxx] + host_flags + inc + ["-c", os.path.join(CSRC, "vl_host.cpp")]),
         ("vl_api.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_api.cu")]),
         ("vl_step_f64.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_step_f64.cu")]),
-        ("vl_step_lp.o", [nvcc] + cu_flags + inc + ["-c", os.path.join(CSRC, "vl_step_lp.cu")]),
+        ("vl_step_lp.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_step_lp.cu")]),
         ("vl_batch.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_batch.cu")]),
         ("vl_nn.o", [nvcc] + cu_flags + inc + ["-c", os.path.join(CSRC, "vl_nn.cu")]),
         ("vl_noalloc.o", [nvcc] + cu_flags + ["-fmad=false"] + inc + ["-c", os.path.join(CSRC, "vl_noalloc.cu")]),

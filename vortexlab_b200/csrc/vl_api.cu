@@ -634,7 +634,9 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   P.link_n = P.nlinkblk;
   P.bulk_b0 = 0;
   P.bulk_n = P.ny;
-  P.pairs = 4;
+  // cells per thread of the narrow bulk kernel: 2 for FP32 (its 4-cell form needs twice the
+  // registers and ran slower on the box), 4 for the 16-bit formats
+  P.pairs = precision == VL_F32 ? 2 : 4;
   staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;

@@ -1,6 +1,8 @@
 // Reduced-precision step kernels: FP32 storage, IEEE FP16 storage of f_i - w_i and the custom
 // 16-bit storage of f_i - w_i (c16), all with FP32 collision arithmetic; the force accumulation and
-// every reduction stay in FP64.
+// every reduction stay in FP64. Compiled without multiply-add contraction like the FP64 kernels:
+// the narrow collision states its fused multiply-adds with intrinsics, and every other expression
+// (link rules, decoding) then rounds the same way in every kernel that evaluates it.
 #include "vl_launch_impl.cuh"
 
 namespace vl {

@@ -69,13 +69,21 @@ def window_values(cd, cl, dt, end, win, steady):
     return float(np.mean(cdw)), float(signal.crossing_frequency(clw, dt) or 0.0)
 
 
-def settled(cd, cl, dt, rule: StopRule):
+def settled(cd, cl, dt, rule: StopRule, cache=None):
     """Whether the run whose history is (cd, cl) has settled; with the statistics of its last
-    window (c_D, St, steady) when it has, else None."""
+    window (c_D, St, steady) when it has, else None. `cache` (a dict kept per run) reuses the
+    window length from the lift spectrum for `spectrum_units / 2` convective units."""
     n = len(cd)
     if n * dt < rule.min_units:
         return None
-    win, steady = _window(cd, cl, dt, rule)
+    if cache is not None and "win" in cache and (n - cache["at"]) * dt < 0.5 * rule.spectrum_units:
+        win, steady = cache["win"], cache["steady"]
+        if not (np.isfinite(cd[-1]) and np.isfinite(cl[-1])):
+            return None
+    else:
+        win, steady = _window(cd, cl, dt, rule)
+        if cache is not None:
+            cache.update(win=win, steady=steady, at=n)
     if win is None:
         return None
     hop = max(1, win // 2)
@@ -137,8 +145,9 @@ def plain_arm(cases, rule: StopRule, max_units=100.0, check_units=2.0, log=None)
         ref = reference(cd, cl, dt, rule)
         stop = None
         if np.all(np.isfinite(cd)):
+            cache = {}
             for end, secs in marks:
-                r = settled(cd[:end], cl[:end], dt, rule)
+                r = settled(cd[:end], cl[:end], dt, rule, cache)
                 if r is not None:
                     stop = dict(steps=end, units=end * dt, seconds=secs, cd=r[0], st=r[1], steady=r[2])
                     break
@@ -150,46 +159,53 @@ def plain_arm(cases, rule: StopRule, max_units=100.0, check_units=2.0, log=None)
 
 
 def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chunk_global=None):
-    """Runs a built batch (every tunnel added with max_units of steps) and stops each tunnel when
-    the rule holds on its own history, read incrementally from the device between runs. Returns
-    per-tunnel dicts (stop or None, steps run, finite) and the host seconds spent in the checks."""
+    """Runs a built batch (every tunnel added with max_units of steps, all starting at step 0) and
+    stops each tunnel when the rule holds on its own history, read incrementally from the device
+    between runs. A running tunnel's step is the batch's global step; a non-finite force record
+    marks it diverged. Returns per-tunnel dicts (stop or None, steps run, finite) and the host
+    seconds spent in the checks."""
     nt = len(cases)
     spu = np.array([c.tunnel.steps_per_unit() for c in cases])
     dt = 1.0 / spu
     every = np.maximum(1, (check_units * spu).astype(np.int64))   # steps between a tunnel's checks
     if chunk_global is None:
         chunk_global = int(every.min())
+    ends = [int(b.info(k)["steps"]) for k in range(nt)]
     hist = [np.zeros((0, 2)) for _ in range(nt)]
+    caches = [dict() for _ in range(nt)]
     next_check = every.copy()
     active = set(range(nt))
     result = [dict(stop=None, steps=0, finite=True) for _ in range(nt)]
     host_s = 0.0
-    total = max(b.info(k)["steps"] for k in range(nt))
+    total = max(ends)
     while active and b.global_step() < total:
         b.run(int(chunk_global))
         t0 = time.perf_counter()
+        s = b.global_step()
         for k in sorted(active):
-            t, nonfinite, _ = b.status(k)
-            if nonfinite:
-                result[k].update(finite=False, steps=int(t))
+            t = min(s, ends[k])
+            if t < next_check[k] and t < ends[k]:
+                continue
+            new = b.force_history_range(k, len(hist[k]), t - len(hist[k]))
+            if len(new):
+                hist[k] = np.concatenate([hist[k], new])
+            next_check[k] = t + every[k]
+            result[k]["steps"] = t
+            if not np.all(np.isfinite(new)):
+                result[k]["finite"] = False
                 active.discard(k)
                 continue
-            if t < next_check[k] and t < b.info(k)["steps"]:
-                continue
-            new = b.force_history_range(k, len(hist[k]), int(t) - len(hist[k]))
-            hist[k] = np.concatenate([hist[k], new]) if len(new) else hist[k]
-            next_check[k] = t + every[k]
             tn = cases[k].tunnel
             cd, cl = _coeff(hist[k], tn.u, tn.d)
-            r = settled(cd, cl, dt[k], rule)
+            r = settled(cd, cl, dt[k], rule, caches[k])
             if r is not None:
-                result[k].update(stop=dict(steps=int(t), units=float(t * dt[k]), cd=r[0], st=r[1], steady=r[2]))
-                if t < b.info(k)["steps"]:
-                    b.set_steps(k, int(t))
+                result[k].update(stop=dict(steps=t, units=float(t * dt[k]), cd=r[0], st=r[1], steady=r[2]))
+                if t < ends[k]:
+                    b.set_steps(k, t)
+                    ends[k] = t
                 active.discard(k)
-            elif t >= b.info(k)["steps"]:
+            elif t >= ends[k]:
                 active.discard(k)
-            result[k]["steps"] = int(t)
         host_s += time.perf_counter() - t0
     for k in range(nt):
         t, nonfinite, _ = b.status(k)
