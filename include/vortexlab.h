@@ -220,6 +220,12 @@ int vl_sim_get_schedule(const vl_sim* s);
  * bit-identical whatever the setting. No reference counterpart (the reference updates one cell
  * per loop iteration, src/sim.rs:700-735). */
 int vl_sim_set_cells_per_thread(vl_sim* s, int cells);
+/* FP32 and 16-bit storage: 1 (the default) = the bulk kernel streams the populations it reads into
+ * shared memory with asynchronous bulk copies (a ring of stages filled by one producer thread per
+ * block), where every row and plane is a whole number of 16-byte units and the multi-cell form
+ * applies; 0 = it loads them directly. Results are bit-identical either way. No reference
+ * counterpart. */
+int vl_sim_set_bulk_copies(vl_sim* s, int on);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the
  * fastest. ms (may be NULL) receives the milliseconds per step of the VL_SCHEDULE_COUNT

@@ -3,7 +3,8 @@
 With FP32 or 16-bit storage the bulk kernel updates 4 or 2 neighbouring cells per thread where the
 row length allows: vector loads and stores of each population plane, the x-shifted planes
 completed by a warp shuffle (and a memory read at the warp's edges and the periodic wrap), the
-collision on packed FP32 pairs. Every lane performs the one-cell kernel's operations, so all forms
+collision on packed FP32 pairs; where rows are whole 16-byte units it reads the planes from
+shared-memory copies that asynchronous bulk copies fill (the bulk-copy-fed kernel). Every lane performs the one-cell kernel's operations, so all forms
 must give bit-identical populations, on every link rule and on grids whose rows end inside a warp,
 in the two-kernel and the staged step. The link kernel collides boundary nodes with the same
 operators, so the schedules agree with each other bit for bit as well.
@@ -27,12 +28,16 @@ def _domains():
         # 122 cells per row (a row ends inside a warp), TRT, inlet, absorbing outlet, moving body
         "tunnel_like": S.tunnel_like(radiating=True),
         "tunnel_walls": S.tunnel_like(radiating=False),
+        # 128 cells per row: whole 16-byte units in every format, so the bulk-copy-fed kernel runs
+        # on every link rule
+        "tunnel_128": S.tunnel_like(nx=128, radiating=True),
     }
 
 
-def _run(d, prec, schedule, cells, steps):
+def _run(d, prec, schedule, cells, steps, copies=True):
     sim = S.product_sim(d, precision=prec)
     sim.set_cells_per_thread(cells)
+    sim.set_bulk_copies(copies)
     sim.schedule = schedule
     nx, ny = d["nx"], d["ny"]
     sim.record(steps)
@@ -59,9 +64,9 @@ def test_two_cell_kernel_matches_one_cell_kernel(gpu, prec, name):
     steps = 150
     out = {}
     for schedule in ("concurrent", "staged"):
-        for cells in (4, 2, 1):
-            out[(schedule, cells)] = _run(d, prec, schedule, cells, steps)
-    ref_f, ref_h = out[("concurrent", 1)]
+        for cells, copies in ((4, True), (4, False), (2, True), (2, False), (1, False)):
+            out[(schedule, cells, copies)] = _run(d, prec, schedule, cells, steps, copies)
+    ref_f, ref_h = out[("concurrent", 1, False)]
     assert np.isfinite(ref_f).all()
     bad = []
     for key, (f, h) in out.items():

@@ -656,6 +656,10 @@ class Sim:
         for the 16-bit formats)."""
         check(lib.vl_sim_set_cells_per_thread(self._h, cells))
 
+    def set_bulk_copies(self, on: bool):
+        """FP32 / 16-bit storage: stream the bulk kernel's loads through shared memory (default)."""
+        check(lib.vl_sim_set_bulk_copies(self._h, int(bool(on))))
+
     def autotune(self, steps_each: int = 8):
         """Times the four kernel schedules without advancing the state; keeps the fastest.
         Returns {schedule: ms per step}."""

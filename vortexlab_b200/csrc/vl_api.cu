@@ -215,6 +215,16 @@ struct vl_sim {
     return VL_OK;
   }
 
+  int set_bulk_copies(int on) {
+    if ((on != 0) != (P.stream != 0) && gexec) {
+      VL_CUDA(cudaStreamSynchronize(stream));
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    P.stream = on ? 1 : 0;
+    return VL_OK;
+  }
+
   int set_schedule(int sc) {
     if (sc < 0 || sc >= VL_SCHEDULE_COUNT) return fail(VL_EINVAL, "schedule must be 0, 1, 2 or 3");
     if (sc != schedule && gexec) {
@@ -637,6 +647,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   // cells per thread of the narrow bulk kernel: 2 for FP32 (its 4-cell form needs twice the
   // registers and ran slower on the box), 4 for the 16-bit formats
   P.pairs = precision == VL_F32 ? 2 : 4;
+  P.stream = 1;
   staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;
@@ -1287,6 +1298,11 @@ int vl_sim_set_schedule(vl_sim* s, int schedule) {
 }
 
 int vl_sim_get_schedule(const vl_sim* s) { return s ? s->schedule : VL_EINVAL; }
+
+int vl_sim_set_bulk_copies(vl_sim* s, int on) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  return s->set_bulk_copies(on);
+}
 
 int vl_sim_set_cells_per_thread(vl_sim* s, int cells) {
   if (!s) return fail(VL_EINVAL, "null sim");

@@ -110,6 +110,9 @@ struct StepParams {
   // narrow storage: the most cells of a row the bulk kernel's threads update (1, 2 or 4; fewer
   // where the row length is not a multiple, one with a body force)
   int pairs;
+  // narrow storage: 1 = the bulk kernel reads the populations through bulk copies into shared
+  // memory where the rows allow it (vl_stream.cuh), 0 = directly
+  int stream;
 };
 
 struct alignas(16) LinkRecDev {

@@ -7,6 +7,7 @@
 #include "vl_device.cuh"
 #include "vl_launch.hpp"
 #include "vl_pair.cuh"
+#include "vl_stream.cuh"
 
 namespace vl {
 
@@ -30,10 +31,45 @@ struct LaunchImpl {
       return 1;
     }
   }
+  // The bulk-copy-fed kernel: narrow storage, a multi-cell form, and rows and planes that are whole
+  // 16-byte units (every copy aligned). Persistent CTAs, two per SM.
+  static int sm_count() {
+    static int n = 0;
+    if (!n) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+      if (n <= 0) n = 148;
+    }
+    return n;
+  }
+  template <int V, int CK, int STAGED>
+  static void launch_stream(const StepParams& p, const S* a, S* b, cudaStream_t s, int rows) {
+    using G = stream::Geometry<S, V>;
+    static bool ready = false;
+    if (!ready) {
+      cudaFuncSetAttribute(k_bulk_stream<S, V, CK, STAGED>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM_BYTES);
+      ready = true;
+    }
+    const long long units = (long long)rows * ((p.nx + G::TW - 1) / G::TW);
+    const long long cap = 2LL * sm_count();
+    const unsigned grid = (unsigned)(units < cap ? units : cap);
+    if (grid) k_bulk_stream<S, V, CK, STAGED><<<grid, stream::kThreads, G::SMEM_BYTES, s>>>(p, a, b);
+  }
   template <int CK, int STAGED>
   static void launch_bulk(const StepParams& p, const S* a, S* b, cudaStream_t s) {
     const int r1 = p.bulk_b0 + p.bulk_n < p.ny ? p.bulk_b0 + p.bulk_n : p.ny;
     const int v = group_width<CK>(p);
+    if constexpr (!std::is_same<S, double>::value && CK != 2) {
+      if (v > 1 && p.stream && (p.nx * (int)sizeof(S)) % 16 == 0 && ((size_t)p.ns * sizeof(S)) % 16 == 0 &&
+          r1 > p.bulk_b0) {
+        if (v == 4)
+          launch_stream<4, CK, STAGED>(p, a, b, s, r1 - p.bulk_b0);
+        else
+          launch_stream<2, CK, STAGED>(p, a, b, s, r1 - p.bulk_b0);
+        return;
+      }
+    }
     for (int r = p.bulk_b0; r < r1; r += 65535) {
       StepParams q = p;
       q.bulk_b0 = r;

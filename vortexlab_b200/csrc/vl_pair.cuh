@@ -78,17 +78,20 @@ struct GroupIO;
 template <>
 struct GroupIO<float, 2> {
   using Word = float2;
-  static __device__ __forceinline__ Word ld(const float* p) { return __ldg(reinterpret_cast<const float2*>(p)); }
+  template <bool SM>
+  static __device__ __forceinline__ Word ld(const float* p) {
+    return SM ? *reinterpret_cast<const float2*>(p) : __ldg(reinterpret_cast<const float2*>(p));
+  }
   static __device__ __forceinline__ void st(float* p, Word w) { *reinterpret_cast<float2*>(p) = w; }
   static __device__ __forceinline__ void dec(int, Word w, float2* o) { o[0] = w; }
   static __device__ __forceinline__ void left(int, Word v, bool edge, const float* ep, float2* o) {
     float up = __shfl_up_sync(0xffffffffu, v.y, 1);
-    if (edge) up = __ldg(ep);
+    if (edge) up = *ep;
     o[0] = make_float2(up, v.x);
   }
   static __device__ __forceinline__ void right(int, Word v, bool edge, const float* ep, float2* o) {
     float dn = __shfl_down_sync(0xffffffffu, v.x, 1);
-    if (edge) dn = __ldg(ep);
+    if (edge) dn = *ep;
     o[0] = make_float2(v.y, dn);
   }
   static __device__ __forceinline__ Word enc(int, const float2* f) { return f[0]; }
@@ -97,7 +100,10 @@ struct GroupIO<float, 2> {
 template <>
 struct GroupIO<float, 4> {
   using Word = float4;
-  static __device__ __forceinline__ Word ld(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+  template <bool SM>
+  static __device__ __forceinline__ Word ld(const float* p) {
+    return SM ? *reinterpret_cast<const float4*>(p) : __ldg(reinterpret_cast<const float4*>(p));
+  }
   static __device__ __forceinline__ void st(float* p, Word w) { *reinterpret_cast<float4*>(p) = w; }
   static __device__ __forceinline__ void dec(int, Word w, float2* o) {
     o[0] = make_float2(w.x, w.y);
@@ -105,29 +111,33 @@ struct GroupIO<float, 4> {
   }
   static __device__ __forceinline__ void left(int, Word v, bool edge, const float* ep, float2* o) {
     float up = __shfl_up_sync(0xffffffffu, v.w, 1);
-    if (edge) up = __ldg(ep);
+    if (edge) up = *ep;
     o[0] = make_float2(up, v.x);
     o[1] = make_float2(v.y, v.z);
   }
   static __device__ __forceinline__ void right(int, Word v, bool edge, const float* ep, float2* o) {
     float dn = __shfl_down_sync(0xffffffffu, v.x, 1);
-    if (edge) dn = __ldg(ep);
+    if (edge) dn = *ep;
     o[0] = make_float2(v.y, v.z);
     o[1] = make_float2(v.w, dn);
   }
   static __device__ __forceinline__ Word enc(int, const float2* f) { return make_float4(f[0].x, f[0].y, f[1].x, f[1].y); }
 };
 
+// One stored 16-bit value (a generic load: the pointer may be in global or shared memory).
 template <class S>
 __device__ __forceinline__ unsigned ld16(const S* p) {
-  return (unsigned)__ldg(reinterpret_cast<const unsigned short*>(p));
+  return (unsigned)*reinterpret_cast<const unsigned short*>(p);
 }
 
 template <class S>
 struct GroupIO<S, 2> {
   using Word = unsigned;
   using C = Codec16<S>;
-  static __device__ __forceinline__ Word ld(const S* p) { return __ldg(reinterpret_cast<const unsigned*>(p)); }
+  template <bool SM>
+  static __device__ __forceinline__ Word ld(const S* p) {
+    return SM ? *reinterpret_cast<const unsigned*>(p) : __ldg(reinterpret_cast<const unsigned*>(p));
+  }
   static __device__ __forceinline__ void st(S* p, Word w) { *reinterpret_cast<unsigned*>(p) = w; }
   static __device__ __forceinline__ void dec(int i, Word w, float2* o) { o[0] = C::dec(i, w); }
   // low half: the previous lane's high half (or the value at `ep`); high half: the own low half
@@ -149,7 +159,10 @@ template <class S>
 struct GroupIO<S, 4> {
   using Word = uint2;
   using C = Codec16<S>;
-  static __device__ __forceinline__ Word ld(const S* p) { return __ldg(reinterpret_cast<const uint2*>(p)); }
+  template <bool SM>
+  static __device__ __forceinline__ Word ld(const S* p) {
+    return SM ? *reinterpret_cast<const uint2*>(p) : __ldg(reinterpret_cast<const uint2*>(p));
+  }
   static __device__ __forceinline__ void st(S* p, Word w) { *reinterpret_cast<uint2*>(p) = w; }
   static __device__ __forceinline__ void dec(int i, Word w, float2* o) {
     o[0] = C::dec(i, w.x);
@@ -196,20 +209,27 @@ struct PairTask {
   int* bad;
   unsigned long long* bad_t;
   const unsigned long long* t_now;
+  // shared-memory sources (bulk-copy fed kernel): plane i of the row is at stage + i * seg, its
+  // element 0 holding cell x0t - halo
+  const void* stage;
+  int seg, x0t, halo;
 };
 
-template <class S, int V, int SHIFT>
-__device__ __forceinline__ void pull_group(const S* __restrict__ row, int i, int x0, int xl, int nx, int lane, bool in,
-                                           float2 (*f)[9]) {
+// The pull of plane i for the thread's group: `src` is where the source row's values are read
+// (global memory, or a shared-memory copy indexed by the same x), `grow` the source row in global
+// memory (read at the periodic wrap).
+template <class S, int V, int SHIFT, bool SM>
+__device__ __forceinline__ void pull_group(const S* __restrict__ src, const S* __restrict__ grow, int i, int x0, int xl,
+                                           int nx, int lane, bool in, float2 (*f)[9]) {
   using IO = GroupIO<S, V>;
   float2 o[V / 2];
-  const typename IO::Word v = IO::ld(row + xl);
+  const typename IO::Word v = IO::template ld<SM>(src + xl);
   if (SHIFT == 0)
     IO::dec(i, v, o);
   else if (SHIFT < 0)
-    IO::left(i, v, lane == 0, row + (x0 == 0 ? nx - 1 : x0 - 1), o);
+    IO::left(i, v, lane == 0, x0 == 0 ? grow + (nx - 1) : src + (x0 - 1), o);
   else
-    IO::right(i, v, in && (lane == 31 || x0 + V >= nx), row + (x0 + V >= nx ? 0 : x0 + V), o);
+    IO::right(i, v, in && (lane == 31 || x0 + V >= nx), x0 + V >= nx ? grow : src + (x0 + V), o);
 #pragma unroll
   for (int p = 0; p < V / 2; ++p) f[p][i] = o[p];
 }
@@ -218,7 +238,7 @@ __device__ __forceinline__ float& cell_of(float2 (*f)[9], int c, int i) {
   return (c & 1) ? f[c >> 1][i].y : f[c >> 1][i].x;
 }
 
-template <class S, int V, int STAGED>
+template <class S, int V, int STAGED, bool SM = false>
 __device__ __forceinline__ void group_update(const PairTask& t, const S* __restrict__ a, S* __restrict__ b) {
   using IO = GroupIO<S, V>;
   const int nx = t.nx, ny = t.ny, y = t.y;
@@ -235,15 +255,21 @@ __device__ __forceinline__ void group_update(const PairTask& t, const S* __restr
 #pragma unroll
   for (int c = 0; c < V; ++c) fl[c] = (int)((flw >> (8 * c)) & 0xffu);
   float2 f[V / 2][9];
-  pull_group<S, V, 0>(a + rc, 0, x0, xl, nx, lane, in, f);
-  pull_group<S, V, -1>(a + 1u * ns + rc, 1, x0, xl, nx, lane, in, f);
-  pull_group<S, V, 0>(a + 2u * ns + rm, 2, x0, xl, nx, lane, in, f);
-  pull_group<S, V, 1>(a + 3u * ns + rc, 3, x0, xl, nx, lane, in, f);
-  pull_group<S, V, 0>(a + 4u * ns + rp, 4, x0, xl, nx, lane, in, f);
-  pull_group<S, V, -1>(a + 5u * ns + rm, 5, x0, xl, nx, lane, in, f);
-  pull_group<S, V, 1>(a + 6u * ns + rm, 6, x0, xl, nx, lane, in, f);
-  pull_group<S, V, 1>(a + 7u * ns + rp, 7, x0, xl, nx, lane, in, f);
-  pull_group<S, V, -1>(a + 8u * ns + rp, 8, x0, xl, nx, lane, in, f);
+  const S* g[9] = {a + rc, a + 1u * ns + rc, a + 2u * ns + rm, a + 3u * ns + rc, a + 4u * ns + rp,
+                   a + 5u * ns + rm, a + 6u * ns + rm, a + 7u * ns + rp, a + 8u * ns + rp};
+  const S* sr[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i)
+    sr[i] = SM ? (const S*)t.stage + (i * t.seg + t.halo - t.x0t) : g[i];
+  pull_group<S, V, 0, SM>(sr[0], g[0], 0, x0, xl, nx, lane, in, f);
+  pull_group<S, V, -1, SM>(sr[1], g[1], 1, x0, xl, nx, lane, in, f);
+  pull_group<S, V, 0, SM>(sr[2], g[2], 2, x0, xl, nx, lane, in, f);
+  pull_group<S, V, 1, SM>(sr[3], g[3], 3, x0, xl, nx, lane, in, f);
+  pull_group<S, V, 0, SM>(sr[4], g[4], 4, x0, xl, nx, lane, in, f);
+  pull_group<S, V, -1, SM>(sr[5], g[5], 5, x0, xl, nx, lane, in, f);
+  pull_group<S, V, 1, SM>(sr[6], g[6], 6, x0, xl, nx, lane, in, f);
+  pull_group<S, V, 1, SM>(sr[7], g[7], 7, x0, xl, nx, lane, in, f);
+  pull_group<S, V, -1, SM>(sr[8], g[8], 8, x0, xl, nx, lane, in, f);
   int k[V];
   if (STAGED) {
     const unsigned lt = (1u << lane) - 1u;

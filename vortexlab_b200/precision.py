@@ -47,7 +47,9 @@ def square_tunnel(d=60, re=150.0, u=0.05, units=70.0, discard=40.0, precisions=P
         st = series.stats(discard)
         i0 = int(discard / series.dt)
         out[p] = dict(cd_mean=st.cd_mean, cd_max=float(np.max(series.cd[i0:])), cl_max=float(np.max(series.cl[i0:])),
-                      cl_rms=st.cl_rms, st=st.st, st_crossings=st.st_crossings, periodic=st.periodic,
+                      cl_rms=st.cl_rms, st=st.st, st_crossings=st.st_crossings,
+                      st_spectrum=float(signal.dominant_frequency(series.cl[i0:], series.dt)[0]),
+                      periodic=st.periodic,
                       steps=len(series.cd), grid=tn.grid(), seconds=time.perf_counter() - t0)
         ch.close()
     return out
