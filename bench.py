@@ -28,13 +28,19 @@ sys.path.insert(0, ROOT)
 BOX = dict(nx=8192, ny=4096, seed=0x5EED0001, fraction=0.05, tau=0.55, u=0.05)
 BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36, "f16c": 36}
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes per node update of the bulk kernel from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum of one launch of the 2048 x 2048 box divided by the nodes it updates:
-# interior nodes for the two-kernel step, all fluid nodes for the staged step; see
-# profiles/k_bulk_k_links_f64_disk_box.md and profiles/k_links_stage_k_bulk_staged_f64_disk_box.md),
-# per (precision, staged). Scaled to a full launch by nodes.
-NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3, ("f64", True): 140.2}
-NCU_TRAFFIC_SOURCE = "ncu dram__bytes_read.sum + dram__bytes_write.sum of one 2048x2048 launch, scaled by nodes"
+# DRAM bytes per node update of the bulk kernel from ncu, per (precision, staged):
+# dram__bytes_read.sum + dram__bytes_write.sum of both launches of one staged step of the
+# 4096 x 2048 box (7,968,653 fluid nodes; 624.1 MB read + 486.2 MB written, 1,110.3 MB), and of one
+# launch of the two-kernel step on the 2048 x 2048 box (interior nodes), divided by the nodes the
+# kernel updates; scaled to the headline box by nodes. Writes still dirty in L2 when a launch ends
+# are not counted (up to the 126 MB L2, about 3 % of a 4096 x 2048 step). See
+# profiles/k_bulk_dram_traffic_f64.md.
+NCU_DRAM_BYTES_PER_LU = {("f64", False): 139.3, ("f64", True): 139.33}
+NCU_TRAFFIC_SOURCE = {
+    True: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one staged step (both launches) of the 4096x2048 "
+          "box, per fluid node, scaled by nodes",
+    False: "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 2048x2048 box, per interior "
+           "node, scaled by nodes"}
 # steps of the full-size parity check against the oracle (about 3 s of oracle time on 16 threads)
 PARITY_STEPS = 20
 
@@ -312,7 +318,7 @@ def bulk_roofline(prec, staged, fluid, interior, steps, link_ms, bulk_ms, total_
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
             "traffic": None if traffic is None else round(traffic * bulk_nodes),
-            "traffic_source": None if traffic is None else NCU_TRAFFIC_SOURCE,
+            "traffic_source": None if traffic is None else NCU_TRAFFIC_SOURCE[staged],
             "kernel": ("k_bulk (staged: all fluid nodes; both launches of a step, with the second link "
                        "part beside them)") if staged else "k_bulk (interior nodes)",
             "bytes_per_node_update": bpl,
