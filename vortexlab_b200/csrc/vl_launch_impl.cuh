@@ -31,8 +31,9 @@ struct LaunchImpl {
       return 1;
     }
   }
-  // The bulk-copy-fed kernel: narrow storage, a multi-cell form, and rows and planes that are whole
-  // 16-byte units (every copy aligned). Persistent CTAs, two per SM.
+  // The bulk-copy-fed kernel: narrow storage, a multi-cell form, a row length that is a multiple of
+  // 16 cells and a plane stride of whole 16-byte units (every copy aligned). Persistent CTAs, two
+  // per SM.
   static int sm_count() {
     static int n = 0;
     if (!n) {
@@ -61,8 +62,7 @@ struct LaunchImpl {
     const int r1 = p.bulk_b0 + p.bulk_n < p.ny ? p.bulk_b0 + p.bulk_n : p.ny;
     const int v = group_width<CK>(p);
     if constexpr (!std::is_same<S, double>::value && CK != 2) {
-      if (v > 1 && p.stream && (p.nx * (int)sizeof(S)) % 16 == 0 && ((size_t)p.ns * sizeof(S)) % 16 == 0 &&
-          r1 > p.bulk_b0) {
+      if (v > 1 && p.stream && p.nx % 16 == 0 && ((size_t)p.ns * sizeof(S)) % 16 == 0 && r1 > p.bulk_b0) {
         if (v == 4)
           launch_stream<4, CK, STAGED>(p, a, b, s, r1 - p.bulk_b0);
         else
