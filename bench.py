@@ -376,8 +376,10 @@ def run_vortexlab(args):
     sim.init((1.0, BOX["u"], 0.0))
     if prec != "f64" and args.cells:
         sim.set_cells_per_thread(args.cells)
-    if prec != "f64" and args.no_bulk_copies:
-        sim.set_bulk_copies(False)
+    if prec != "f64" and args.bulk_copies:
+        sim.set_bulk_copies(True)
+    if args.prefetch:
+        sim.set_prefetch_rows(args.prefetch)
     tune = sim.autotune(8) if args.schedule == "auto" else None
     if args.schedule != "auto":
         sim.schedule = args.schedule
@@ -438,7 +440,7 @@ def run_vortexlab(args):
         "run": {"timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
                 "schedule": sim.schedule, "autotune_ms_per_step": tune, "setup_s": round(setup_s, 2),
                 "cells_per_thread": (args.cells or "default") if prec != "f64" else 1,
-                "bulk_copies": prec != "f64" and not args.no_bulk_copies},
+                "bulk_copies": prec != "f64" and args.bulk_copies, "prefetch_rows": args.prefetch},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(d2h / args.steps), "seconds": round(e2e_s, 4),
@@ -497,8 +499,10 @@ def main():
     ap.add_argument("--no-parity", action="store_true")
     ap.add_argument("--schedule", default="auto", choices=["auto", "concurrent", "links-first", "bulk-first", "staged"])
     ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
-    ap.add_argument("--no-bulk-copies", action="store_true",
-                    help="narrow storage: load the populations directly (Sim.set_bulk_copies(False))")
+    ap.add_argument("--bulk-copies", action="store_true",
+                    help="narrow storage: stream the bulk kernel's loads through shared memory (Sim.set_bulk_copies)")
+    ap.add_argument("--prefetch", type=int, default=0,
+                    help="rows ahead the bulk kernel's blocks prefetch into the L2 (Sim.set_prefetch_rows)")
     ap.add_argument("--cells", type=int, default=0, choices=[0, 1, 2, 4],
                     help="narrow storage: the most bulk cells per thread (Sim.set_cells_per_thread; 0: the "
                          "library's default)")

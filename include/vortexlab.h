@@ -226,6 +226,11 @@ int vl_sim_set_cells_per_thread(vl_sim* s, int cells);
  * applies; 0 = it loads them directly. Results are bit-identical either way. No reference
  * counterpart. */
 int vl_sim_set_bulk_copies(vl_sim* s, int on);
+/* Each block of the bulk kernel asks the L2 to fetch (bulk prefetch) the rows its tile will read
+ * `rows` output rows later (0, the default: none), so that the blocks then running find them in
+ * the L2. Only where every row and plane is a whole number of 16-byte units (VL_EUNSUPPORTED
+ * otherwise, and no prefetch). Results are unchanged. No reference counterpart. */
+int vl_sim_set_prefetch_rows(vl_sim* s, int rows);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the
  * fastest. ms (may be NULL) receives the milliseconds per step of the VL_SCHEDULE_COUNT

@@ -34,10 +34,18 @@ def _domains():
     }
 
 
-def _run(d, prec, schedule, cells, steps, copies=True):
+def _aligned(d, prec):
+    elem = {"f64": 8, "f32": 4, "f16s": 2, "f16c": 2}[prec]
+    return d["nx"] * elem % 16 == 0
+
+
+def _run(d, prec, schedule, cells, steps, copies=True, prefetch=0):
     sim = S.product_sim(d, precision=prec)
-    sim.set_cells_per_thread(cells)
-    sim.set_bulk_copies(copies)
+    if prec != "f64":
+        sim.set_cells_per_thread(cells)
+        sim.set_bulk_copies(copies)
+    if prefetch:
+        sim.set_prefetch_rows(prefetch)
     sim.schedule = schedule
     nx, ny = d["nx"], d["ny"]
     sim.record(steps)
@@ -66,6 +74,8 @@ def test_two_cell_kernel_matches_one_cell_kernel(gpu, prec, name):
     for schedule in ("concurrent", "staged"):
         for cells, copies in ((4, True), (4, False), (2, True), (2, False), (1, False)):
             out[(schedule, cells, copies)] = _run(d, prec, schedule, cells, steps, copies)
+        if _aligned(d, prec):
+            out[(schedule, 4, "prefetch")] = _run(d, prec, schedule, 4, steps, False, prefetch=7)
     ref_f, ref_h = out[("concurrent", 1, False)]
     assert np.isfinite(ref_f).all()
     bad = []
@@ -90,3 +100,14 @@ def test_odd_row_length_uses_the_one_cell_kernel(gpu):
     a, _ = _run(d, "f32", "staged", 2, 100)
     b, _ = _run(d, "f32", "staged", 1, 100)
     assert np.array_equal(a, b) and np.isfinite(a).all()
+
+
+@pytest.mark.parametrize("name", ["disk_box_640x200", "tunnel_128"])
+def test_prefetch_changes_nothing(gpu, name):
+    """The L2 prefetch of later rows' tiles is a hint only: FP64 populations and forces are the same
+    with and without it, in the two-kernel and the staged step."""
+    d = _domains()[name]
+    for schedule in ("concurrent", "staged"):
+        a, ha = _run(d, "f64", schedule, 1, 100)
+        b, hb = _run(d, "f64", schedule, 1, 100, prefetch=5)
+        assert np.array_equal(a, b) and np.array_equal(ha, hb), schedule

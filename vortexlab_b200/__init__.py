@@ -656,6 +656,10 @@ class Sim:
         for the 16-bit formats)."""
         check(lib.vl_sim_set_cells_per_thread(self._h, cells))
 
+    def set_prefetch_rows(self, rows: int):
+        """Bulk-kernel blocks ask the L2 for the rows their tile reads `rows` rows later (0: off)."""
+        check(lib.vl_sim_set_prefetch_rows(self._h, rows))
+
     def set_bulk_copies(self, on: bool):
         """FP32 / 16-bit storage: stream the bulk kernel's loads through shared memory (default)."""
         check(lib.vl_sim_set_bulk_copies(self._h, int(bool(on))))

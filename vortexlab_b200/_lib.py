@@ -111,6 +111,7 @@ def _declare(L):
         "vl_sim_set_dp_probe": (i, [vp, d, d, d, d]),
         "vl_sim_last_step_ms": (i, [vp, P(f)]),
         "vl_sim_step_profiled": (i, [vp, u64, P(d), P(d), P(d)]),
+        "vl_sim_set_prefetch_rows": (i, [vp, i]),
         "vl_sim_set_bulk_copies": (i, [vp, i]),
         "vl_sim_set_cells_per_thread": (i, [vp, i]),
         "vl_sim_set_schedule": (i, [vp, i]),

@@ -215,6 +215,21 @@ struct vl_sim {
     return VL_OK;
   }
 
+  int set_prefetch_rows(int rows) {
+    if (rows < 0 || rows > 4096) return fail(VL_EINVAL, "prefetch rows must be in 0..4096");
+    // a prefetch must start on a 16-byte boundary and cover whole 16-byte units
+    const size_t row_bytes = (size_t)P.nx * L->elem, plane_bytes = (size_t)P.ns * L->elem;
+    const int ok = row_bytes % 16 == 0 && plane_bytes % 16 == 0 && ((size_t)vl::kBlock * L->elem) % 16 == 0;
+    const int want = ok ? rows : 0;
+    if (want != P.prefetch_rows && gexec) {
+      VL_CUDA(cudaStreamSynchronize(stream));
+      cudaGraphExecDestroy(gexec);
+      gexec = nullptr;
+    }
+    P.prefetch_rows = want;
+    return ok || rows == 0 ? VL_OK : fail(VL_EUNSUPPORTED, "rows are not whole 16-byte units: no prefetch");
+  }
+
   int set_bulk_copies(int on) {
     if ((on != 0) != (P.stream != 0) && gexec) {
       VL_CUDA(cudaStreamSynchronize(stream));
@@ -647,7 +662,8 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
   // cells per thread of the narrow bulk kernel: 2 for FP32 (its 4-cell form needs twice the
   // registers and ran slower on the box), 4 for the 16-bit formats
   P.pairs = precision == VL_F32 ? 2 : 4;
-  P.stream = 1;
+  P.stream = 0;
+  P.prefetch_rows = 0;
   staged_split(d, lnode, s->split_links, s->split_rows);
   P.bdesc = s->d_bdesc;
   P.warp_bfirst = s->d_wbfirst;
@@ -1298,6 +1314,11 @@ int vl_sim_set_schedule(vl_sim* s, int schedule) {
 }
 
 int vl_sim_get_schedule(const vl_sim* s) { return s ? s->schedule : VL_EINVAL; }
+
+int vl_sim_set_prefetch_rows(vl_sim* s, int rows) {
+  if (!s) return fail(VL_EINVAL, "null sim");
+  return s->set_prefetch_rows(rows);
+}
 
 int vl_sim_set_bulk_copies(vl_sim* s, int on) {
   if (!s) return fail(VL_EINVAL, "null sim");

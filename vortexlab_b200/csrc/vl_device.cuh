@@ -113,7 +113,28 @@ struct StepParams {
   // narrow storage: 1 = the bulk kernel reads the populations through bulk copies into shared
   // memory where the rows allow it (vl_stream.cuh), 0 = directly
   int stream;
+  // rows ahead whose tile a block of the bulk kernel asks the L2 to fetch (0: none; used where
+  // every row of every plane is a whole number of 16-byte units)
+  int prefetch_rows;
 };
+
+// One thread of a bulk-kernel block asks the L2 to fetch, for the block's tile of `cells` cells
+// starting at x0, the nine plane rows that the tile of output row `y` will read (bulk prefetch:
+// no registers and no shared memory held; the later loads then hit the L2). The caller has
+// checked that every row of every plane is a whole number of 16-byte units.
+template <class S>
+__device__ __forceinline__ void prefetch_tile(const S* a, unsigned ns, int nx, int ny, int y, int x0, int cells) {
+  const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
+  const int end = min(x0 + cells, nx);
+  if (end <= x0) return;
+  const unsigned bytes = (unsigned)(end - x0) * (unsigned)sizeof(S);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const int r = (i == 2 || i == 5 || i == 6) ? ym : ((i == 4 || i == 7 || i == 8) ? yp : y);
+    const S* src = a + (size_t)i * ns + (size_t)r * nx + x0;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+  }
+}
 
 struct alignas(16) LinkRecDev {
   double q, cu6, uw0, uw1, rho;
@@ -480,6 +501,10 @@ __global__ void __launch_bounds__(kBlock) k_bulk(const __grid_constant__ StepPar
   const int y = (int)blockIdx.y + p.bulk_b0;
   const int x = (int)blockIdx.x * kBlock + (int)threadIdx.x;
   const int tile = y * p.tiles_per_row + (int)blockIdx.x;
+  if (p.prefetch_rows && threadIdx.x == 0) {
+    const int yf = y + p.prefetch_rows;
+    prefetch_tile(a, p.ns, nx, ny, yf >= ny ? yf - ny : yf, (int)blockIdx.x * kBlock, kBlock);
+  }
   if (!STAGED && x >= nx) return;
   const bool in = x < nx;
   const unsigned idx = (unsigned)(y * nx + x);

@@ -358,6 +358,10 @@ __global__ void __launch_bounds__(kBlock, group_min_blocks<S, V>()) k_bulkv(cons
   t.ny = p.ny;
   t.y = (int)blockIdx.y + p.bulk_b0;
   t.xw = (int)blockIdx.x * (V * kBlock) + (int)(threadIdx.x >> 5) * (32 * V);
+  if (p.prefetch_rows && threadIdx.x == 0) {
+    const int yf = t.y + p.prefetch_rows;
+    prefetch_tile(a, p.ns, t.nx, t.ny, yf >= t.ny ? yf - t.ny : yf, (int)blockIdx.x * (V * kBlock), V * kBlock);
+  }
   if (t.xw >= t.nx) return;   // the whole warp is past the row end
   t.ns = p.ns;
   t.flag = p.flag;
