@@ -7,7 +7,8 @@
 //
 // MODE 0: FP64 (no rounding); 1: IEEE half; 2: the custom 16-bit format of the GPU path (sign,
 // 3-bit exponent, 12-bit mantissa, exponent bias 9: 2^(e-9) (1 + m/4096), m 2^-20 below 2^-8,
-// saturating at 0.49994); 3: 16-bit fixed point with a step of 2^-18. Prints c_D max / mean,
+// saturating at 0.49994); 3: 16-bit fixed point with a step of 2^-18; 4: 16-bit fixed point with
+// steps 2^-19 (rest), 2^-18 (axis directions), 2^-19 (diagonals). Prints c_D max / mean,
 // c_L max / min, St (dominant lift frequency) over the last `window` convective units and the
 // total mass.
 #include "vl_oracle.cpp"
@@ -35,9 +36,9 @@ double round_custom(double d) {
   return (double)(z * 0x1p118f);
 }
 
-double round_fixed(double d) {
-  const double q = std::min(std::max(std::nearbyint(d * 0x1p18), -32768.0), 32767.0);
-  return q * 0x1p-18;
+double round_fixed(double d, int k) {
+  const double q = std::min(std::max(std::nearbyint(std::ldexp(d, k)), -32768.0), 32767.0);
+  return std::ldexp(q, -k);
 }
 
 }  // namespace
@@ -74,7 +75,10 @@ int main(int argc, char** argv) {
         for (int i = 0; i < 9; ++i)
           for (size_t idx = th * N / nt; idx < (th + 1) * N / nt; ++idx) {
             const double d = pa[i * N + idx] - kW[i];
-            const double q = mode == 1 ? (double)(_Float16)(float)d : mode == 2 ? round_custom(d) : round_fixed(d);
+            const double q = mode == 1   ? (double)(_Float16)(float)d
+                             : mode == 2 ? round_custom(d)
+                             : mode == 3 ? round_fixed(d, 18)
+                                         : round_fixed(d, i == 0 ? 19 : (i < 5 ? 18 : 19));
             pa[i * N + idx] = kW[i] + q;
           }
       });
