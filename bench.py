@@ -378,7 +378,7 @@ def run_vortexlab(args):
         sim.set_cells_per_thread(args.cells)
     if prec != "f64" and args.bulk_copies:
         sim.set_bulk_copies(True)
-    if args.prefetch:
+    if args.prefetch >= 0:
         sim.set_prefetch_rows(args.prefetch)
     tune = sim.autotune(8) if args.schedule == "auto" else None
     if args.schedule != "auto":
@@ -440,7 +440,7 @@ def run_vortexlab(args):
         "run": {"timing": "CUDA events around every kernel on the stream it runs on, max over ranks",
                 "schedule": sim.schedule, "autotune_ms_per_step": tune, "setup_s": round(setup_s, 2),
                 "cells_per_thread": (args.cells or "default") if prec != "f64" else 1,
-                "bulk_copies": prec != "f64" and args.bulk_copies, "prefetch_rows": args.prefetch},
+                "bulk_copies": prec != "f64" and args.bulk_copies, "prefetch_rows": args.prefetch if args.prefetch >= 0 else "default"},
         "roofline": roofline,
         "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": round(h2d / args.steps),
                 "d2h_bytes_per_step": round(d2h / args.steps), "seconds": round(e2e_s, 4),
@@ -501,8 +501,9 @@ def main():
     ap.add_argument("--box", default=None, help="NXxNY: a smaller box of the same kind (profiling cases)")
     ap.add_argument("--bulk-copies", action="store_true",
                     help="narrow storage: stream the bulk kernel's loads through shared memory (Sim.set_bulk_copies)")
-    ap.add_argument("--prefetch", type=int, default=0,
-                    help="rows ahead the bulk kernel's blocks prefetch into the L2 (Sim.set_prefetch_rows)")
+    ap.add_argument("--prefetch", type=int, default=-1,
+                    help="rows ahead the bulk kernel's blocks prefetch into the L2 (Sim.set_prefetch_rows; "
+                         "-1: the library's default)")
     ap.add_argument("--cells", type=int, default=0, choices=[0, 1, 2, 4],
                     help="narrow storage: the most bulk cells per thread (Sim.set_cells_per_thread; 0: the "
                          "library's default)")

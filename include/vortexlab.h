@@ -227,9 +227,9 @@ int vl_sim_set_cells_per_thread(vl_sim* s, int cells);
  * counterpart. */
 int vl_sim_set_bulk_copies(vl_sim* s, int on);
 /* Each block of the bulk kernel asks the L2 to fetch (bulk prefetch) the rows its tile will read
- * `rows` output rows later (0, the default: none), so that the blocks then running find them in
- * the L2. Only where every row and plane is a whole number of 16-byte units (VL_EUNSUPPORTED
- * otherwise, and no prefetch). Results are unchanged. No reference counterpart. */
+ * `rows` output rows later (0: none), so that the blocks then running find them in the L2.
+ * Default: none for FP64; for the narrow formats about two waves of blocks ahead (2 x SMs blocks).
+ * Results are unchanged. No reference counterpart. */
 int vl_sim_set_prefetch_rows(vl_sim* s, int rows);
 /* Times each schedule for `steps_each` steps on the current state without advancing it (t, the
  * force, the history and the populations of the current state are unchanged) and keeps the
@@ -309,6 +309,9 @@ int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty);
 /* FP32 and 16-bit storage: 2 (the default where every tunnel's row length is even) bulk cells of a
  * row per thread, as vl_sim_set_cells_per_thread, or 1. Results are bit-identical either way. */
 int vl_batch_set_cells_per_thread(vl_batch* b, int cells);
+/* Each bulk block asks the L2 to fetch the rows of the tile `tiles` places later in the tile list
+ * (0: none; default 2 x SMs for the narrow formats, none for FP64), as vl_sim_set_prefetch_rows. */
+int vl_batch_set_prefetch_tiles(vl_batch* b, int tiles);
 int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty);
 int vl_batch_set_schedule(vl_batch* b, int schedule);  /* VL_SCHEDULE_* */
 /* Times the tile shapes 256x1, 128x2, 64x4, 32x8 on the current state without advancing it and

@@ -132,6 +132,7 @@ def _declare(L):
         "vl_batch_build": (i, [vp]),
         "vl_batch_size": (i, [vp]),
         "vl_batch_tunnel_info": (i, [vp, i, P(sz), P(sz), P(sz), P(u64)]),
+        "vl_batch_set_prefetch_tiles": (i, [vp, i]),
         "vl_batch_set_cells_per_thread": (i, [vp, i]),
         "vl_batch_set_tile": (i, [vp, i, i]),
         "vl_batch_get_tile": (i, [vp, P(i), P(i)]),

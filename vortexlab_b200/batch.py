@@ -92,6 +92,10 @@ class Batch:
         """FP32 / 16-bit storage: 2 (default where every row length is even) bulk cells per thread, or 1."""
         check(lib.vl_batch_set_cells_per_thread(self._h, cells))
 
+    def set_prefetch_tiles(self, tiles: int):
+        """Bulk blocks prefetch into the L2 the tile `tiles` places ahead in the list (0: off)."""
+        check(lib.vl_batch_set_prefetch_tiles(self._h, tiles))
+
     def autotune(self, steps_each=4):
         """Times the four tile shapes without advancing the tunnels; keeps the fastest."""
         out = np.zeros(4)

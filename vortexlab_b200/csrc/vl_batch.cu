@@ -132,6 +132,7 @@ struct vl_batch {
     VB_CUDA(cudaStreamSynchronize(stream));
     ntiles = (int)tiles_h.size();
     nchunks = (int)chunks_h.size();
+    P.ntiles = ntiles;
     P.tiles = d_tiles;
     P.chunks = d_chunks;
     P.log2_tx = log2_tx;
@@ -478,6 +479,13 @@ int vl_batch_build(vl_batch* b) {
     P.pairs = even ? 1 : 0;
   }
   b->pairs_ok = P.pairs != 0;
+  // narrow formats: each bulk block prefetches into the L2 the tile two waves of blocks ahead
+  P.prefetch_tiles = 0;
+  if (!precision_is_f64(b->prec)) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    P.prefetch_tiles = 2 * sms;
+  }
   b->built = true;
   // The host plans (domains) are no longer needed on the host except their sizes.
   for (auto& pl : b->plans) {
@@ -514,6 +522,17 @@ int vl_batch_set_cells_per_thread(vl_batch* b, int cells) {
   if (want == b->P.pairs) return VL_OK;
   b->P.pairs = want;
   return b->build_lists(false);
+}
+
+int vl_batch_set_prefetch_tiles(vl_batch* b, int tiles) {
+  if (!b || !b->built || tiles < 0) return fail(VL_EINVAL, "bad arguments");
+  if (tiles == b->P.prefetch_tiles) return VL_OK;
+  b->P.prefetch_tiles = tiles;
+  if (b->gexec) {
+    cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+  }
+  return VL_OK;
 }
 
 int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty) {

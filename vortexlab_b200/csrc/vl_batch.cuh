@@ -82,7 +82,24 @@ struct BatchParams {
   // narrow storage with every row length even: the bulk kernel is the two-cell form and a tile is
   // 2 * 2^log2_tx cells wide
   int pairs;
+  int ntiles;                   // tiles in the list
+  int prefetch_tiles;           // a bulk block prefetches into the L2 the tile this far ahead (0: none)
 };
+
+// Threads of a bulk block ask the L2 for the rows of tile `k` of the list (one plane row each).
+template <class S>
+__device__ __forceinline__ void batch_prefetch(const BatchParams& p, const S* A, int k, int width) {
+  if (k >= p.ntiles || (int)threadIdx.x >= 9 * p.ty) return;
+  const int4 td = __ldg(p.tiles + k);
+  const BatchTunnel& T = p.tun[td.x];
+  const int i = (int)threadIdx.x % 9, y = td.y + (int)threadIdx.x / 9;
+  if (y >= T.ny) return;
+  const int ym = y == 0 ? T.ny - 1 : y - 1, yp = y == T.ny - 1 ? 0 : y + 1;
+  const int r = (i == 2 || i == 5 || i == 6) ? ym : ((i == 4 || i == 7 || i == 8) ? yp : y);
+  const int end = min(td.z + width, T.nx);
+  if (end <= td.z) return;
+  prefetch_l2(A + T.pop_off + (size_t)i * T.ns + (size_t)r * T.nx + td.z, (size_t)(end - td.z) * sizeof(S));
+}
 
 // Controls of a tunnel at its step t (src/cases/channel.rs:118-130).
 __device__ __forceinline__ void tunnel_controls(const BatchParams& p, const BatchTunnel& T, unsigned long long t,
@@ -106,6 +123,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
   // Only tunnels that are active for the whole launch are in the tile list (the host rebuilds it
   // when a tunnel finishes), so the tile never checks the tunnel's t, which the link kernel's
   // epilogue may advance concurrently.
+  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 1 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);
   const BatchTunnel& T = p.tun[td.x];
   const int nx = T.nx, ny = T.ny;
@@ -155,6 +173,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
 template <class S, int STAGED>
 __global__ void __launch_bounds__(kBlock) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
+  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 2 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);
   const BatchTunnel& T = p.tun[td.x];
   PairTask t;

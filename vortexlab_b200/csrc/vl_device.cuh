@@ -113,26 +113,30 @@ struct StepParams {
   // narrow storage: 1 = the bulk kernel reads the populations through bulk copies into shared
   // memory where the rows allow it (vl_stream.cuh), 0 = directly
   int stream;
-  // rows ahead whose tile a block of the bulk kernel asks the L2 to fetch (0: none; used where
-  // every row of every plane is a whole number of 16-byte units)
+  // rows ahead whose tile a block of the bulk kernel asks the L2 to fetch (0: none)
   int prefetch_rows;
 };
 
-// One thread of a bulk-kernel block asks the L2 to fetch, for the block's tile of `cells` cells
-// starting at x0, the nine plane rows that the tile of output row `y` will read (bulk prefetch:
-// no registers and no shared memory held; the later loads then hit the L2). The caller has
-// checked that every row of every plane is a whole number of 16-byte units.
+// Asks the L2 to fetch (bulk prefetch: no registers or shared memory held; later loads then hit the
+// L2) the whole 16-byte units inside [p, p + bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+  const uintptr_t b0 = ((uintptr_t)p + 15u) & ~(uintptr_t)15u;
+  const uintptr_t b1 = ((uintptr_t)p + bytes) & ~(uintptr_t)15u;
+  if (b1 > b0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(b0), "r"((unsigned)(b1 - b0)) : "memory");
+}
+
+// The nine plane rows that the tile of `cells` cells at x0 of output row `y` reads, prefetched
+// into the L2 by one thread of a bulk-kernel block some rows ahead of its own.
 template <class S>
 __device__ __forceinline__ void prefetch_tile(const S* a, unsigned ns, int nx, int ny, int y, int x0, int cells) {
   const int ym = y == 0 ? ny - 1 : y - 1, yp = y == ny - 1 ? 0 : y + 1;
   const int end = min(x0 + cells, nx);
   if (end <= x0) return;
-  const unsigned bytes = (unsigned)(end - x0) * (unsigned)sizeof(S);
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
     const int r = (i == 2 || i == 5 || i == 6) ? ym : ((i == 4 || i == 7 || i == 8) ? yp : y);
-    const S* src = a + (size_t)i * ns + (size_t)r * nx + x0;
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+    prefetch_l2(a + (size_t)i * ns + (size_t)r * nx + x0, (size_t)(end - x0) * sizeof(S));
   }
 }
 
