@@ -320,6 +320,19 @@ int vl_batch_autotune(vl_batch* b, int steps_each, double* ms4);
 /* Runs every unfinished tunnel until it has done its steps (max_steps = 0), or at most max_steps
  * global steps. Synchronous. */
 int vl_batch_run(vl_batch* b, uint64_t max_steps);
+/* The same steps enqueued on the batch's stream without waiting for them; vl_batch_wait (or any
+ * call that reads the batch's state) waits. While they run, the host may read the force records
+ * of steps complete at the previous wait (vl_batch_history_copy) and end tunnels
+ * (vl_batch_set_steps with a step at or after the enqueued run's end). */
+int vl_batch_run_async(vl_batch* b, uint64_t max_steps);
+int vl_batch_wait(vl_batch* b);
+/* Force records (fx, fy per step) of n ranges, concatenated into out (2 * sum(counts) doubles):
+ * steps [firsts[i], firsts[i] + counts[i]) of tunnel ks[i]. Every range must lie within the
+ * tunnel's history and before the global step complete at the last wait (records a tunnel has
+ * not written, after it ended, are not defined). Read on a stream of its own, so it does not wait
+ * for a run in flight. No reference counterpart (the on-line stopping rule's input). */
+int vl_batch_history_copy(vl_batch* b, int n, const int* ks, const uint64_t* firsts, const uint64_t* counts,
+                          double* out);
 int vl_batch_last_run_ms(vl_batch* b, float* ms);
 int vl_batch_global_step(const vl_batch* b, uint64_t* s);
 int vl_batch_launch_count(const vl_batch* b, uint64_t* out);
@@ -333,8 +346,9 @@ int vl_batch_force_history_range(vl_batch* b, int k, uint64_t first, uint64_t ma
 /* FP64 populations of tunnel k (reference layout, 9 * nx * ny values), its flags, its state hash. */
 int vl_batch_download(vl_batch* b, int k, double* out);
 /* Ends tunnel k after `steps` steps instead of the count it was added with (which stays the upper
- * bound and sizes its force history); allowed while the tunnel has not run past `steps`. Lets a
- * caller stop each tunnel at a moment it picks from the tunnel's own force history. */
+ * bound and sizes its force history); allowed while the tunnel has not run past `steps`, counting
+ * the steps of a run in flight, which the change follows on the stream. Lets a caller stop each
+ * tunnel at a moment it picks from the tunnel's own force history. */
 int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps);
 /* Density and velocity of every cell of tunnel k at its current step (solids (1, 0, 0)), FP64,
  * row-major n = nx * ny values each: Sim::macros (src/sim.rs:527-536) over the whole grid. */

@@ -157,6 +157,47 @@ def test_batch_set_steps_matches_a_shorter_run(gpu):
         assert np.array_equal(b.force_history(k), ref.force_history(k)), k
 
 
+def test_async_runs_and_history_copy(gpu):
+    """Chunks enqueued with run_async, tunnels ended while a chunk is in flight and histories read
+    beside it (vl_batch_history_copy) give the states and records of synchronous runs with the same
+    ends; a range past the steps complete at the last wait is refused."""
+    V = gpu
+    from vortexlab_b200.batch import Batch
+    cases = _cases(V)
+    ref = Batch("f32")
+    for k, c in enumerate(cases):
+        ref.add(c.tunnel.spec(c.body), 30 if k == 1 else c.steps)
+    ref.build()
+    ref.run()
+    b = Batch("f32")
+    for c in cases:
+        b.add(c.tunnel.spec(c.body), c.steps)
+    b.build()
+    b.run_async(10)
+    b.wait()
+    b.run_async(20)                       # steps 10..30 in flight
+    got = b.history_copy([(0, 0, 10), (2, 3, 7), (1, 0, 0)])
+    with pytest.raises(V.VortexError):
+        b.history_copy([(0, 5, 6)])       # step 10 is not complete at the last wait
+    b.set_steps(1, 30)                    # the end of the chunk in flight
+    with pytest.raises(V.VortexError):
+        b.set_steps(3, 29)                # inside the chunk in flight
+    b.run_async()
+    b.wait()
+    assert got[0].shape == (10, 2) and got[2].shape == (0, 2)
+    assert np.array_equal(got[0], ref.force_history(0)[:10])
+    assert np.array_equal(got[1], ref.force_history(2)[3:10])
+    assert b.status(1)[0] == 30
+    for k in range(len(cases)):
+        assert b.state_hash(k) == ref.state_hash(k), k
+        assert np.array_equal(b.force_history(k), ref.force_history(k)), k
+    whole = b.history_copy([(k, 0, cases[k].steps if k != 1 else 30) for k in range(len(cases))])
+    for k in range(len(cases)):
+        assert np.array_equal(whole[k], ref.force_history(k)), k
+    b.close()
+    ref.close()
+
+
 def test_batch_init_from_a_grid_matches_the_host_decode(gpu):
     """vl_batch_init_grid (bilinear sampling and decoding of a coarse grid of normalised fields on
     the device) gives the fields of the host decode followed by vl_batch_init."""

@@ -75,3 +75,90 @@ def test_cached_window_stops_like_the_full_rule():
     assert abs(t_cached - t_full) <= 2.0 + 1e-9
     assert abs(r_cached[0] - r_full[0]) <= 1e-3 * abs(r_full[0])
     assert abs(r_cached[1] - r_full[1]) <= 1e-3 * r_full[1]
+
+
+class _FakeBatch:
+    """Host stand-in for a batch of tunnels with the asynchronous run semantics of the library:
+    run_async advances the global step at once, records become readable after wait, and a tunnel
+    can be ended only at or after the step the enqueued run ends at."""
+
+    def __init__(self, histories, steps):
+        self.h = histories          # per tunnel (n, 2) force records
+        self.steps = list(steps)
+        self.s = 0
+        self.s_done = 0
+        self.run_steps = 0
+
+    def info(self, k):
+        return {"steps": self.steps[k]}
+
+    def run_async(self, n):
+        end = min(max(self.steps), self.s + n)
+        self.run_steps += sum(max(0, min(e, end) - min(e, self.s)) for e in self.steps)
+        self.s = max(self.s, end)
+
+    def wait(self):
+        self.s_done = self.s
+
+    def global_step(self):
+        return self.s
+
+    def history_copy(self, ranges):
+        out = []
+        for k, first, count in ranges:
+            assert first + count <= min(self.s_done, self.steps[k]), (k, first, count, self.s_done)
+            out.append(self.h[k][first:first + count])
+        return out
+
+    def set_steps(self, k, steps):
+        assert steps >= self.s and steps <= self.steps[k]
+        self.steps[k] = steps
+
+    def status(self, k):
+        return min(self.s, self.steps[k]), False, None
+
+
+class _Tun:
+    def __init__(self, spu, u=0.05, d=20.0):
+        self.spu, self.u, self.d = spu, u, d
+
+    def steps_per_unit(self):
+        return self.spu
+
+
+class _Case:
+    def __init__(self, spu):
+        self.tunnel = _Tun(spu)
+
+
+def test_overlapped_batch_checks_stop_each_tunnel_within_a_chunk():
+    """batch_online with a chunk in flight during the checks: each tunnel stops where the rule
+    first holds on its own records (checked every 2 convective units), is ended at the end of the
+    chunk enqueued at that moment, never reads a record that is not complete, and every step it ran
+    is counted."""
+    from vortexlab_b200.online import batch_online
+    rule = StopRule()
+    spus, settles = [300, 600, 450], [10.0, 25.0, 400.0]     # the last never settles in 60 units
+    hist, cases = [], []
+    k_force = 2.0 / (0.05 * 0.05 * 20.0)
+    for spu, st in zip(spus, settles):
+        cd, cl, dt = _history(units=60.0, dt=1.0 / spu, settle=st)
+        hist.append(np.stack([cd / k_force, cl / k_force], axis=1))
+        cases.append(_Case(spu))
+    b = _FakeBatch(hist, [len(h) for h in hist])
+    res, _ = batch_online(b, cases, rule, max_units=60.0, check_units=2.0)
+    chunk = 600
+    for k, (spu, r) in enumerate(zip(spus, res)):
+        cd, cl = hist[k][:, 0] * k_force, hist[k][:, 1] * k_force
+        every = 2 * spu
+        want = None
+        for end in range(every, len(cd) + 1, every):
+            if settled(cd[:end], cl[:end], 1.0 / spu, rule) is not None:
+                want = end
+                break
+        if want is None:
+            assert r["stop"] is None and r["steps"] == len(cd), k
+        else:
+            assert r["stop"]["steps"] == want, (k, r["stop"], want)
+            assert want <= r["steps"] <= want + chunk, (k, r["steps"], want)
+    assert b.run_steps == sum(r["steps"] for r in res)

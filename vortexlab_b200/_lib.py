@@ -132,6 +132,9 @@ def _declare(L):
         "vl_batch_build": (i, [vp]),
         "vl_batch_size": (i, [vp]),
         "vl_batch_tunnel_info": (i, [vp, i, P(sz), P(sz), P(sz), P(u64)]),
+        "vl_batch_run_async": (i, [vp, u64]),
+        "vl_batch_wait": (i, [vp]),
+        "vl_batch_history_copy": (i, [vp, i, P(i), P(u64), P(u64), P(d)]),
         "vl_batch_set_prefetch_tiles": (i, [vp, i]),
         "vl_batch_set_cells_per_thread": (i, [vp, i]),
         "vl_batch_set_tile": (i, [vp, i, i]),

@@ -105,6 +105,29 @@ class Batch:
     def run(self, max_steps: int = 0):
         check(lib.vl_batch_run(self._h, max_steps))
 
+    def run_async(self, max_steps: int = 0):
+        """Enqueues the steps of `run` without waiting for them (`wait` does)."""
+        check(lib.vl_batch_run_async(self._h, max_steps))
+
+    def wait(self):
+        check(lib.vl_batch_wait(self._h))
+
+    def history_copy(self, ranges):
+        """Force records of several tunnels at once: `ranges` is a list of (k, first, count) with
+        every step complete at the last `wait`; returns one (count, 2) array per range. Does not
+        wait for a run in flight."""
+        n = len(ranges)
+        ks = (C.c_int * max(n, 1))(*[r[0] for r in ranges])
+        firsts = (C.c_uint64 * max(n, 1))(*[r[1] for r in ranges])
+        counts = (C.c_uint64 * max(n, 1))(*[r[2] for r in ranges])
+        out = np.empty((max(sum(r[2] for r in ranges), 1), 2))
+        check(lib.vl_batch_history_copy(self._h, n, ks, firsts, counts, _dp(out)))
+        res, at = [], 0
+        for r in ranges:
+            res.append(out[at:at + r[2]])
+            at += r[2]
+        return res
+
     def last_run_ms(self) -> float:
         out = C.c_float()
         check(lib.vl_batch_last_run_ms(self._h, C.byref(out)))

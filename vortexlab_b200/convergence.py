@@ -212,9 +212,11 @@ def warm_comparison(net, cases, refs=None, precision="f32", tol=0.005):
     return dict(summary=summary, rows=rows)
 
 
-def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0, schedule="concurrent", cells=2):
+def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0, schedule="concurrent", cells=2,
+               prefetch=-1):
     """The full seeded batch: MLUPS of the whole run (or of its first `max_steps` global steps).
-    `cells`: bulk cells per thread (2: the two-cell kernel where every row length is even)."""
+    `cells`: bulk cells per thread (2: the two-cell kernel where every row length is even);
+    `prefetch`: L2 prefetch distance in tiles (-1: the library default)."""
     from .batch import Batch, seeded_tunnels
     cases = seeded_tunnels(seed=seed, count=count, precision=precision)
     b = Batch(precision)
@@ -225,6 +227,8 @@ def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0, schedul
     setup = time.perf_counter() - t0
     b.schedule = schedule
     b.set_cells_per_thread(cells)
+    if prefetch >= 0:
+        b.set_prefetch_tiles(prefetch)
     tune = b.autotune(3)
     b.run(max_steps)
     ms = b.last_run_ms()
@@ -234,7 +238,7 @@ def throughput(seed=0x5EED0004, count=256, precision="f32", max_steps=0, schedul
         lu += b.info(k)["fluid_nodes"] * t
     out = dict(tunnels=count, precision=precision, global_steps=b.global_step(), lattice_updates=lu,
                seconds=ms * 1e-3, mlups=lu / (ms * 1e-3) / 1e6, tile=b.tile, schedule=schedule, cells_per_thread=cells,
-               autotune_ms_per_step=tune,
+               prefetch_tiles=prefetch, autotune_ms_per_step=tune,
                setup_s=setup, launches=b.launch_count(),
                diverged=[k for k in range(count) if b.status(k)[1]])
     b.close()
@@ -249,6 +253,7 @@ if __name__ == "__main__":
         print(json.dumps(throughput(max_steps=int(sys.argv[2]) if len(sys.argv) > 2 else 0,
                                     schedule=sys.argv[3] if len(sys.argv) > 3 else "concurrent",
                                     precision=sys.argv[4] if len(sys.argv) > 4 else "f32",
-                                    cells=int(sys.argv[5]) if len(sys.argv) > 5 else 2), default=float))
+                                    cells=int(sys.argv[5]) if len(sys.argv) > 5 else 2,
+                                    prefetch=int(sys.argv[6]) if len(sys.argv) > 6 else -1), default=float))
     else:
         print(json.dumps(study(subset=int(sys.argv[2]) if len(sys.argv) > 2 else 32), default=float, indent=1))

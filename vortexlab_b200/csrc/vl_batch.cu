@@ -89,7 +89,12 @@ struct vl_batch {
   uint64_t launches = 0;
   cudaGraphExec_t gexec = nullptr;
   std::vector<int4> tiles_h, chunks_h;   // host copies of the current work lists
+  std::vector<char> listed;              // which tunnels the current work lists hold
+  int listed_tx = -1, listed_ty = -1, listed_pairs = -1;
   bool timed = false;
+  bool in_flight = false;                // a run was enqueued and not yet waited for
+  uint64_t s_done = 0;                   // global steps complete on the device at the last wait
+  cudaStream_t copy = nullptr;           // history reads beside a run in flight
 
   ~vl_batch() {
     cudaSetDevice(device);
@@ -103,6 +108,7 @@ struct vl_batch {
       if (e) cudaEventDestroy(e);
     if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
+    if (copy) cudaStreamDestroy(copy);
   }
 
   const void* a() const { return buf[s & 1]; }
@@ -128,8 +134,14 @@ struct vl_batch {
       VB_CUDA(cudaMalloc(&d_tiles, tiles_cap * sizeof(int4)));
     }
     VB_CUDA(cudaMemcpyAsync(d_tiles, tiles_h.data(), tiles_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+    // Pageable host to device: the host vectors are staged before the calls return, and the
+    // copies are ordered after any run still in flight on the stream, which reads the old lists.
     VB_CUDA(cudaMemcpyAsync(d_chunks, chunks_h.data(), chunks_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
-    VB_CUDA(cudaStreamSynchronize(stream));
+    listed.assign(tun.size(), 0);
+    for (size_t k = 0; k < tun.size(); ++k) listed[k] = all || s < tun[k].steps;
+    listed_tx = log2_tx;
+    listed_ty = ty;
+    listed_pairs = P.pairs;
     ntiles = (int)tiles_h.size();
     nchunks = (int)chunks_h.size();
     P.ntiles = ntiles;
@@ -142,6 +154,14 @@ struct vl_batch {
       gexec = nullptr;
     }
     return VL_OK;
+  }
+
+  // Whether the work lists already hold exactly the tunnels active at step s.
+  bool lists_current() const {
+    if (listed.size() != tun.size() || listed_tx != log2_tx || listed_ty != ty || listed_pairs != P.pairs) return false;
+    for (size_t k = 0; k < tun.size(); ++k)
+      if ((bool)listed[k] != (s < tun[k].steps)) return false;
+    return true;
   }
 
   // The staged step reads the boundary nodes' own populations from d_ownc; after anything other
@@ -200,7 +220,8 @@ struct vl_batch {
     return VL_OK;
   }
 
-  int run(uint64_t max_steps) {
+  // Enqueues the steps of a run on the stream without waiting for them.
+  int enqueue_run(uint64_t max_steps) {
     VB_CUDA(cudaSetDevice(device));
     uint64_t end_all = 0;
     for (auto& T : tun) end_all = std::max<uint64_t>(end_all, T.steps);
@@ -210,7 +231,7 @@ struct vl_batch {
       uint64_t seg_end = stop;
       for (auto& T : tun)
         if (T.steps > s) seg_end = std::min<uint64_t>(seg_end, T.steps);
-      int rc = build_lists(false);
+      int rc = lists_current() ? VL_OK : build_lists(false);
       if (rc) return rc;
       if ((rc = prepare_steps())) return rc;
       while (s < seg_end) {
@@ -230,9 +251,23 @@ struct vl_batch {
       own_ok = schedule == 3;
     }
     VB_CUDA(cudaEventRecord(ev1, stream));
-    VB_CUDA(cudaStreamSynchronize(stream));
-    timed = true;
+    in_flight = true;
+    timed = false;
     return VL_OK;
+  }
+
+  int wait() {
+    VB_CUDA(cudaSetDevice(device));
+    VB_CUDA(cudaStreamSynchronize(stream));
+    if (in_flight) timed = true;
+    in_flight = false;
+    s_done = s;
+    return VL_OK;
+  }
+
+  int run(uint64_t max_steps) {
+    int rc = enqueue_run(max_steps);
+    return rc ? rc : wait();
   }
 
   // Times the candidate tile shapes on the current state without advancing it and keeps the
@@ -423,6 +458,7 @@ int vl_batch_build(vl_batch* b) {
   VB_CUDA(cudaMalloc(&b->d_hist, std::max<unsigned long long>(hist, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   VB_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+  VB_CUDA(cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking));
   VB_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   VB_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
   VB_CUDA(cudaEventCreate(&b->ev0));
@@ -562,6 +598,38 @@ int vl_batch_run(vl_batch* b, uint64_t max_steps) {
   return b->run(max_steps);
 }
 
+int vl_batch_run_async(vl_batch* b, uint64_t max_steps) {
+  if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
+  return b->enqueue_run(max_steps);
+}
+
+int vl_batch_wait(vl_batch* b) {
+  if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
+  return b->wait();
+}
+
+int vl_batch_history_copy(vl_batch* b, int n, const int* ks, const uint64_t* firsts, const uint64_t* counts,
+                          double* out) {
+  if (!b || !b->built || n < 0 || (n && (!ks || !firsts || !counts || !out))) return fail(VL_EINVAL, "bad arguments");
+  for (int i = 0; i < n; ++i) {
+    const int k = ks[i];
+    if (k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "tunnel index out of range");
+    if (firsts[i] > b->steps[k] || counts[i] > b->steps[k] - firsts[i])
+      return fail(VL_EINVAL, "range past the tunnel's force history");
+    if (firsts[i] + counts[i] > b->s_done) return fail(VL_EINVAL, "range past the steps complete at the last wait");
+  }
+  VB_CUDA(cudaSetDevice(b->device));
+  double* o = out;
+  for (int i = 0; i < n; ++i) {
+    if (counts[i])
+      VB_CUDA(cudaMemcpyAsync(o, b->d_hist + 2 * (b->tun[ks[i]].hist_off + firsts[i]), counts[i] * 2 * sizeof(double),
+                              cudaMemcpyDeviceToHost, b->copy));
+    o += 2 * counts[i];
+  }
+  VB_CUDA(cudaStreamSynchronize(b->copy));
+  return VL_OK;
+}
+
 int vl_batch_last_run_ms(vl_batch* b, float* ms) {
   if (!b || !ms || !b->timed) return fail(VL_EINVAL, "no run timed yet");
   VB_CUDA(cudaEventElapsedTime(ms, b->ev0, b->ev1));
@@ -582,8 +650,7 @@ int vl_batch_launch_count(const vl_batch* b, uint64_t* out) {
 
 static int pull_state(vl_batch* b, int k, vl::BatchState* st) {
   VB_CUDA(cudaMemcpyAsync(st, b->d_st + k, sizeof *st, cudaMemcpyDeviceToHost, b->stream));
-  VB_CUDA(cudaStreamSynchronize(b->stream));
-  return VL_OK;
+  return b->wait();
 }
 
 int vl_batch_status(vl_batch* b, int k, uint64_t* t, int* nonfinite, double* force2) {
@@ -647,8 +714,9 @@ int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps) {
   if (steps > b->steps[k]) return fail(VL_EINVAL, "a tunnel cannot run longer than the steps it was added with");
   if (steps == T.steps) return VL_OK;
   T.steps = steps;
+  // ordered after a run in flight, which still reads the old end (the host value is staged
+  // before the call returns)
   VB_CUDA(cudaMemcpyAsync(&b->d_tun[k].steps, &T.steps, sizeof T.steps, cudaMemcpyHostToDevice, b->stream));
-  VB_CUDA(cudaStreamSynchronize(b->stream));
   if (b->gexec) {       // the captured steps may cover the new end: capture again
     cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;

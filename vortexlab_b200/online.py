@@ -160,10 +160,14 @@ def plain_arm(cases, rule: StopRule, max_units=100.0, check_units=2.0, log=None)
 
 def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chunk_global=None):
     """Runs a built batch (every tunnel added with max_units of steps, all starting at step 0) and
-    stops each tunnel when the rule holds on its own history, read incrementally from the device
-    between runs. A running tunnel's step is the batch's global step; a non-finite force record
-    marks it diverged. Returns per-tunnel dicts (stop or None, steps run, finite) and the host
-    seconds spent in the checks."""
+    stops each tunnel when the rule holds on its own history. The device runs the next chunk of
+    global steps while the host reads the records of the chunk just finished (one copy for every
+    tunnel due a check) and applies the rule, so a tunnel found settled at step t is ended at the
+    end of the chunk already enqueued: it runs at most one chunk past its stop, and those steps
+    count in the wall time and in the lattice updates like any other. A running tunnel's step is
+    the batch's global step; a non-finite force record marks it diverged (and ends it). Returns
+    per-tunnel dicts (stop or None, steps run, finite) and the host seconds spent in the checks
+    (overlapped with the device)."""
     nt = len(cases)
     spu = np.array([c.tunnel.steps_per_unit() for c in cases])
     dt = 1.0 / spu
@@ -180,37 +184,52 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
     active = set(range(nt))
     result = [dict(stop=None, steps=0, finite=True) for _ in range(nt)]
     host_s = 0.0
-    total = max(ends)
-    while active and b.global_step() < total:
-        b.run(int(chunk_global))
+
+    def end_at(k, s_next):
+        if s_next < ends[k]:
+            b.set_steps(k, s_next)
+            ends[k] = s_next
+
+    b.run_async(int(chunk_global))
+    while True:
+        b.wait()
+        s_done = b.global_step()
+        more = any(ends[k] > s_done for k in active)
+        if more:
+            b.run_async(int(chunk_global))
+        s_next = b.global_step()
         t0 = time.perf_counter()
-        s = b.global_step()
+        due = []
         for k in sorted(active):
-            t = min(s, ends[k])
+            t = min(s_done, ends[k])
             if t < next_check[k] and t < ends[k]:
                 continue
-            new = b.force_history_range(k, have[k], t - have[k])
+            due.append((k, have[k], t - have[k]))
+        for (k, first, count), new in zip(due, b.history_copy(due) if due else []):
+            t = first + count
             tn = cases[k].tunnel
             ncd, ncl = _coeff(new, tn.u, tn.d)
-            cds[k][have[k]:have[k] + len(new)] = ncd
-            cls[k][have[k]:have[k] + len(new)] = ncl
-            have[k] += len(new)
+            cds[k][first:t] = ncd
+            cls[k][first:t] = ncl
+            have[k] = t
             next_check[k] = t + every[k]
             result[k]["steps"] = t
             if not (np.all(np.isfinite(ncd)) and np.all(np.isfinite(ncl))):
                 result[k]["finite"] = False
                 active.discard(k)
+                end_at(k, s_next)
                 continue
-            r = settled(cds[k][:have[k]], cls[k][:have[k]], dt[k], rule, caches[k])
+            r = settled(cds[k][:t], cls[k][:t], dt[k], rule, caches[k])
             if r is not None:
                 result[k].update(stop=dict(steps=t, units=float(t * dt[k]), cd=r[0], st=r[1], steady=r[2]))
-                if t < ends[k]:
-                    b.set_steps(k, t)
-                    ends[k] = t
                 active.discard(k)
+                end_at(k, s_next)
             elif t >= ends[k]:
                 active.discard(k)
         host_s += time.perf_counter() - t0
+        if not more:
+            break
+    b.wait()
     for k in range(nt):
         t, nonfinite, _ = b.status(k)
         result[k]["steps"] = int(t)
