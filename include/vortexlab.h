@@ -310,7 +310,7 @@ int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty);
  * row per thread, as vl_sim_set_cells_per_thread, or 1. Results are bit-identical either way. */
 int vl_batch_set_cells_per_thread(vl_batch* b, int cells);
 /* Each bulk block asks the L2 to fetch the rows of the tile `tiles` places later in the tile list
- * (0: none; default 2 x SMs for the narrow formats, none for FP64), as vl_sim_set_prefetch_rows. */
+ * (0: none; default 3 x SMs for the narrow formats, none for FP64), as vl_sim_set_prefetch_rows. */
 int vl_batch_set_prefetch_tiles(vl_batch* b, int tiles);
 int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty);
 int vl_batch_set_schedule(vl_batch* b, int schedule);  /* VL_SCHEDULE_* */

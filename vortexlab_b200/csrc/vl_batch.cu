@@ -95,6 +95,8 @@ struct vl_batch {
   bool in_flight = false;                // a run was enqueued and not yet waited for
   uint64_t s_done = 0;                   // global steps complete on the device at the last wait
   cudaStream_t copy = nullptr;           // history reads beside a run in flight
+  double* h_stage = nullptr;             // pinned staging of those reads
+  size_t h_stage_cap = 0;                // doubles
 
   ~vl_batch() {
     cudaSetDevice(device);
@@ -109,6 +111,7 @@ struct vl_batch {
     if (aux) cudaStreamDestroy(aux);
     if (stream) cudaStreamDestroy(stream);
     if (copy) cudaStreamDestroy(copy);
+    if (h_stage) cudaFreeHost(h_stage);
   }
 
   const void* a() const { return buf[s & 1]; }
@@ -515,12 +518,12 @@ int vl_batch_build(vl_batch* b) {
     P.pairs = even ? 1 : 0;
   }
   b->pairs_ok = P.pairs != 0;
-  // narrow formats: each bulk block prefetches into the L2 the tile two waves of blocks ahead
+  // narrow formats: each bulk block prefetches into the L2 the tile three waves of blocks ahead
   P.prefetch_tiles = 0;
   if (!precision_is_f64(b->prec)) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    P.prefetch_tiles = 2 * sms;
+    P.prefetch_tiles = 3 * sms;
   }
   b->built = true;
   // The host plans (domains) are no longer needed on the host except their sizes.
@@ -619,14 +622,26 @@ int vl_batch_history_copy(vl_batch* b, int n, const int* ks, const uint64_t* fir
     if (firsts[i] + counts[i] > b->s_done) return fail(VL_EINVAL, "range past the steps complete at the last wait");
   }
   VB_CUDA(cudaSetDevice(b->device));
-  double* o = out;
+  size_t total = 0;
+  for (int i = 0; i < n; ++i) total += 2 * counts[i];
+  if (total > b->h_stage_cap) {
+    if (b->h_stage) VB_CUDA(cudaFreeHost(b->h_stage));
+    b->h_stage = nullptr;
+    b->h_stage_cap = 0;
+    const size_t cap = std::max<size_t>(total, 1 << 16);
+    VB_CUDA(cudaHostAlloc(&b->h_stage, cap * sizeof(double), cudaHostAllocDefault));
+    b->h_stage_cap = cap;
+  }
+  // one copy per range into pinned memory (asynchronous DMA beside the run), one wait
+  size_t at = 0;
   for (int i = 0; i < n; ++i) {
     if (counts[i])
-      VB_CUDA(cudaMemcpyAsync(o, b->d_hist + 2 * (b->tun[ks[i]].hist_off + firsts[i]), counts[i] * 2 * sizeof(double),
-                              cudaMemcpyDeviceToHost, b->copy));
-    o += 2 * counts[i];
+      VB_CUDA(cudaMemcpyAsync(b->h_stage + at, b->d_hist + 2 * (b->tun[ks[i]].hist_off + firsts[i]),
+                              counts[i] * 2 * sizeof(double), cudaMemcpyDeviceToHost, b->copy));
+    at += 2 * counts[i];
   }
   VB_CUDA(cudaStreamSynchronize(b->copy));
+  if (total) std::memcpy(out, b->h_stage, total * sizeof(double));
   return VL_OK;
 }
 

@@ -48,14 +48,18 @@ class StopRule:
 
 
 def _window(cd, cl, dt, rule):
-    """(window in steps, steady?) from the lift spectrum of the last `spectrum_units`."""
+    """(window in steps, steady?) from the lift spectrum of the last `spectrum_units`. The spectrum
+    is taken of every m-th record (about 64 per convective unit; a shedding period is several
+    units, so the line is far below the decimated Nyquist frequency): the window only needs the
+    period to a fraction of a percent, and the full-rate spectrum costs milliseconds per check."""
     n = min(len(cl), int(rule.spectrum_units / dt))
     if n < 8 or not (np.all(np.isfinite(cl[-n:])) and np.all(np.isfinite(cd[-n:]))):
         return None, False
     seg = cl[-n:]
     if np.std(seg) <= rule.steady_lift * max(abs(float(np.mean(cd[-n:]))), 1e-12):
         return int(rule.steady_units / dt), True
-    f = signal.dominant_frequency(seg, dt)[0]
+    m = max(1, int(1.0 / (64.0 * dt)))
+    f = signal.dominant_frequency(seg[len(seg) % m::m], dt * m)[0]
     if not (f > 0 and np.isfinite(f)):
         return int(rule.steady_units / dt), True
     return max(8, int(rule.periods / f / dt)), False
