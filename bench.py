@@ -275,6 +275,27 @@ def channel_n80(V):
     return out
 
 
+def batched_256(global_steps=1000):
+    """The batched configuration: 256 seeded tunnels (seed 0x5EED0004: ellipses, notched squares,
+    star-convex polygons, D 15-60, Re 50-200, 20 D x 10 D, TRT), FP32 storage, one batch; the
+    first `global_steps` global steps after the tile autotuner, device-timed (CUDA events around
+    the run on its stream). Roofline of the whole step (bulk and link kernels) at 72 B per fluid
+    node update."""
+    from vortexlab_b200.convergence import throughput
+    r = throughput(max_steps=global_steps)
+    peak, peak_kind = hbm_peak()
+    achieved = r["mlups"] * 1e6 * BYTES_PER_LU["f32"] / 1e9
+    return {"workload": "256 seeded tunnels (seed 0x5EED0004), D 15-60, Re 50-200, TRT, f32 populations, "
+                        f"first {r['global_steps']} global steps",
+            "mlups": round(r["mlups"], 1), "seconds": round(r["seconds"], 4),
+            "lattice_updates": int(r["lattice_updates"]), "tile": r["tile"], "schedule": r["schedule"],
+            "cells_per_thread": r["cells_per_thread"], "launches": int(r["launches"]),
+            "diverged": r["diverged"],
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "peak_kind": peak_kind,
+                         "kernel": "whole batched step (bulk and link kernels)", "bytes_per_node_update": 72}}
+
+
 def time_to_converged():
     """The second half of the headline metric on a bounded sample: time to converged c_D and St of
     the fast form (FP32, batched, learned warm start with the shipped network, uniform-start
@@ -467,6 +488,7 @@ def run_vortexlab(args):
     if rank == 0 and world == 1 and not args.no_extras:
         line["precision_f32"] = box_variant(V, "f32", args.steps, args.warmup)
         line["precision_f16s"] = box_variant(V, "f16s", args.steps, args.warmup)
+        line["batched_256"] = batched_256()
         line["channel_n80"] = channel_n80(V)
         line["time_to_converged"] = time_to_converged()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -170,8 +170,11 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
 // The two-cell form of k_batch_bulk for narrow storage (every tunnel's row length even): a tile is
 // 2 * 2^log2_tx cells x ty rows, thread t of the tile updates the pair at 2 (t mod 2^log2_tx) of
 // row t / 2^log2_tx; a warp covers 64 cells of one row (2^log2_tx >= 32).
+#ifndef VL_BATCH_PAIR_MIN_BLOCKS
+#define VL_BATCH_PAIR_MIN_BLOCKS 1
+#endif
 template <class S, int STAGED>
-__global__ void __launch_bounds__(kBlock) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
+__global__ void __launch_bounds__(kBlock, VL_BATCH_PAIR_MIN_BLOCKS) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
   if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 2 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);

@@ -343,9 +343,12 @@ __device__ __forceinline__ void group_update(const PairTask& t, const S* __restr
 
 // Resident blocks per SM the register allocation targets: 16-bit storage 5 (V = 2) or 3 (V = 4);
 // FP32 4 or 2 (its V = 4 threads keep 144 bytes of loads in flight each).
+#ifndef VL_F32_PAIR_MIN_BLOCKS
+#define VL_F32_PAIR_MIN_BLOCKS 4
+#endif
 template <class S, int V>
 constexpr int group_min_blocks() {
-  return sizeof(S) == 4 ? (V == 2 ? 4 : 2) : (V == 2 ? 5 : 3);
+  return sizeof(S) == 4 ? (V == 2 ? VL_F32_PAIR_MIN_BLOCKS : 2) : (V == 2 ? 5 : 3);
 }
 
 // One sim: block (t, y) updates the V * kBlock cells of tile t of row y (from p.bulk_b0).
