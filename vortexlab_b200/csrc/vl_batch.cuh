@@ -170,11 +170,18 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
 // The two-cell form of k_batch_bulk for narrow storage (every tunnel's row length even): a tile is
 // 2 * 2^log2_tx cells x ty rows, thread t of the tile updates the pair at 2 (t mod 2^log2_tx) of
 // row t / 2^log2_tx; a warp covers 64 cells of one row (2^log2_tx >= 32).
+// Resident blocks per SM the two-cell batch kernel is compiled for: FP32 5 (48 registers, a few
+// spilled; left to itself the compiler takes 76-80 registers, 3 blocks per SM, and the batch
+// streams 13 % slower), 16-bit 4.
 #ifndef VL_BATCH_PAIR_MIN_BLOCKS
-#define VL_BATCH_PAIR_MIN_BLOCKS 1
+#define VL_BATCH_PAIR_MIN_BLOCKS 5
 #endif
+template <class S>
+constexpr int batch_pair_min_blocks() {
+  return sizeof(S) == 4 ? VL_BATCH_PAIR_MIN_BLOCKS : 4;
+}
 template <class S, int STAGED>
-__global__ void __launch_bounds__(kBlock, VL_BATCH_PAIR_MIN_BLOCKS) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
+__global__ void __launch_bounds__(kBlock, batch_pair_min_blocks<S>()) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
   if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 2 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);

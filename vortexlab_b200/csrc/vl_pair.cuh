@@ -342,9 +342,10 @@ __device__ __forceinline__ void group_update(const PairTask& t, const S* __restr
 }
 
 // Resident blocks per SM the register allocation targets: 16-bit storage 5 (V = 2) or 3 (V = 4);
-// FP32 4 or 2 (its V = 4 threads keep 144 bytes of loads in flight each).
+// FP32 5 (V = 2: 48 registers, no spills; 4 blocks measured 0.2 % slower, 6 blocks spill and ran
+// 2 % slower) or 2 (its V = 4 threads keep 144 bytes of loads in flight each).
 #ifndef VL_F32_PAIR_MIN_BLOCKS
-#define VL_F32_PAIR_MIN_BLOCKS 4
+#define VL_F32_PAIR_MIN_BLOCKS 5
 #endif
 template <class S, int V>
 constexpr int group_min_blocks() {

@@ -188,15 +188,20 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
     active = set(range(nt))
     result = [dict(stop=None, steps=0, finite=True) for _ in range(nt)]
     host_s = 0.0
+    parts = dict(wait_s=0.0, copy_s=0.0, end_s=0.0)
 
     def end_at(k, s_next):
         if s_next < ends[k]:
+            t1 = time.perf_counter()
             b.set_steps(k, s_next)
+            parts["end_s"] += time.perf_counter() - t1
             ends[k] = s_next
 
     b.run_async(int(chunk_global))
     while True:
+        t1 = time.perf_counter()
         b.wait()
+        parts["wait_s"] += time.perf_counter() - t1
         s_done = b.global_step()
         more = any(ends[k] > s_done for k in active)
         if more:
@@ -209,7 +214,10 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
             if t < next_check[k] and t < ends[k]:
                 continue
             due.append((k, have[k], t - have[k]))
-        for (k, first, count), new in zip(due, b.history_copy(due) if due else []):
+        t1 = time.perf_counter()
+        got = b.history_copy(due) if due else []
+        parts["copy_s"] += time.perf_counter() - t1
+        for (k, first, count), new in zip(due, got):
             t = first + count
             tn = cases[k].tunnel
             ncd, ncl = _coeff(new, tn.u, tn.d)
@@ -239,6 +247,7 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
         result[k]["steps"] = int(t)
         if nonfinite:
             result[k]["finite"] = False
+    batch_online.last_parts = parts
     return result, host_s
 
 
@@ -272,6 +281,7 @@ def fast_arm(cases, rule: StopRule, net=None, precision="f32", max_units=100.0, 
     run_s = time.perf_counter() - t_run
     lu = sum(_lattice_cells(c) * r["steps"] for c, r in zip(cases, res))
     info = dict(tile=b.tile, autotune_ms_per_step=tune, init_s=t_init, run_s=run_s, check_host_s=host_s,
+                check_parts={k: round(v, 3) for k, v in batch_online.last_parts.items()},
                 device_ms=b.last_run_ms(), lattice_updates=lu)
     b.close()
     for r in res:
