@@ -304,7 +304,10 @@ int vl_batch_add_channel(vl_batch* b, const vl_channel_spec* spec, uint64_t step
 int vl_batch_build(vl_batch* b);
 int vl_batch_size(const vl_batch* b);
 int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_t* fluid_nodes, uint64_t* steps);
-/* Bulk tile shape: 2^log2_tx cells x ty rows = 256 cells (32 <= 2^log2_tx <= 256). */
+/* Bulk tile shape: 2^log2_tx cells x ty rows = 256 cells (32 <= 2^log2_tx <= 256), times the
+ * bulk cells per thread; or (5, 0): the packed layout, 8 consecutive warp segments (32 cells times
+ * the cells per thread, of one row each) of a tunnel's rows laid end to end, so that only the last
+ * segment of each row runs past the row end. */
 int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty);
 /* FP32 and 16-bit storage: 2 (the default where every tunnel's row length is even) bulk cells of a
  * row per thread, as vl_sim_set_cells_per_thread, or 1. Results are bit-identical either way. */
@@ -314,9 +317,12 @@ int vl_batch_set_cells_per_thread(vl_batch* b, int cells);
 int vl_batch_set_prefetch_tiles(vl_batch* b, int tiles);
 int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty);
 int vl_batch_set_schedule(vl_batch* b, int schedule);  /* VL_SCHEDULE_* */
-/* Times the tile shapes 256x1, 128x2, 64x4, 32x8 on the current state without advancing it and
- * keeps the fastest; ms4 (may be NULL) receives milliseconds per step for each. */
+/* Times the tile shapes 256x1, 128x2, 64x4, 32x8 and the packed layout on the current state
+ * without advancing it and keeps the fastest; ms4 (may be NULL) receives milliseconds per step for
+ * the four row shapes. */
 int vl_batch_autotune(vl_batch* b, int steps_each, double* ms4);
+/* The same; ms (may be NULL) receives up to n of the five times (row shapes, then packed). */
+int vl_batch_autotune_layouts(vl_batch* b, int steps_each, double* ms, int n);
 /* Runs every unfinished tunnel until it has done its steps (max_steps = 0), or at most max_steps
  * global steps. Synchronous. */
 int vl_batch_run(vl_batch* b, uint64_t max_steps);

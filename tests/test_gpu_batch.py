@@ -31,9 +31,10 @@ def test_batched_tunnels_match_single_runs(gpu, prec):
         single.append((ch.sim.state_hash(), ch.sim.history()[:, :2].copy(), ch.sim.populations().copy()))
         ch.close()
     runs = [("256x1", "concurrent", 2), ("64x4", "links-first", 2), ("32x8", "bulk-first", 2),
-            ("128x2", "staged", 2), ("32x8", "staged", 2)]
+            ("128x2", "staged", 2), ("32x8", "staged", 2), ("packed", "concurrent", 2), ("packed", "staged", 2)]
     if prec != "f64":
-        runs += [("256x1", "concurrent", 1), ("128x2", "staged", 1)]
+        runs += [("256x1", "concurrent", 1), ("128x2", "staged", 1), ("packed", "concurrent", 1),
+                 ("packed", "staged", 1)]
     for tile, sched, cells in runs:
         b = Batch(prec)
         for c in cases:

@@ -28,7 +28,7 @@ def _dp(a):
 
 class Batch:
     SCHEDULES = {"concurrent": 0, "links-first": 1, "bulk-first": 2, "staged": 3}
-    TILES = {(8, 1): "256x1", (7, 2): "128x2", (6, 4): "64x4", (5, 8): "32x8"}
+    TILES = {(8, 1): "256x1", (7, 2): "128x2", (6, 4): "64x4", (5, 8): "32x8", (5, 0): "packed"}
 
     def __init__(self, precision="f32"):
         self.precision = precision
@@ -97,9 +97,10 @@ class Batch:
         check(lib.vl_batch_set_prefetch_tiles(self._h, tiles))
 
     def autotune(self, steps_each=4):
-        """Times the four tile shapes without advancing the tunnels; keeps the fastest."""
-        out = np.zeros(4)
-        check(lib.vl_batch_autotune(self._h, steps_each, _dp(out)))
+        """Times the four row tile shapes and the packed layout without advancing the tunnels;
+        keeps the fastest."""
+        out = np.zeros(len(self.TILES))
+        check(lib.vl_batch_autotune_layouts(self._h, steps_each, _dp(out), len(out)))
         return dict(zip(self.TILES.values(), out.tolist()))
 
     def run(self, max_steps: int = 0):

@@ -123,11 +123,18 @@ struct vl_batch {
     tiles_h.clear();
     chunks_h.clear();
     const int tx = (1 << log2_tx) << (P.pairs ? 1 : 0);   // cells per tile row
+    const int seg = 32 << (P.pairs ? 1 : 0);               // packed layout: cells per warp segment
+    const int wpb = vl::kBlock / 32;                       // warp segments per packed tile
     for (size_t k = 0; k < tun.size(); ++k) {
       if (!all && s >= tun[k].steps) continue;
       const vl::BatchTunnel& T = tun[k];
-      for (int y0 = 0; y0 < T.ny; y0 += ty)
-        for (int x0 = 0; x0 < T.nx; x0 += tx) tiles_h.push_back(make_int4((int)k, y0, x0, 0));
+      if (ty == 0) {
+        const int total = T.ny * ((T.nx + seg - 1) / seg);
+        for (int g0 = 0; g0 < total; g0 += wpb) tiles_h.push_back(make_int4((int)k, g0, 0, 0));
+      } else {
+        for (int y0 = 0; y0 < T.ny; y0 += ty)
+          for (int x0 = 0; x0 < T.nx; x0 += tx) tiles_h.push_back(make_int4((int)k, y0, x0, 0));
+      }
       for (int c = 0; c < T.nchunks; ++c) chunks_h.push_back(chunks_all[chunk_first[k] + c]);
     }
     if (tiles_h.size() > tiles_cap) {
@@ -152,6 +159,7 @@ struct vl_batch {
     P.chunks = d_chunks;
     P.log2_tx = log2_tx;
     P.ty = ty;
+    P.packed = ty == 0;
     if (gexec) {
       cudaGraphExecDestroy(gexec);
       gexec = nullptr;
@@ -275,13 +283,15 @@ struct vl_batch {
 
   // Times the candidate tile shapes on the current state without advancing it and keeps the
   // fastest. Shapes: 256 x 1, 128 x 2, 64 x 4, 32 x 8 cells.
-  int autotune(int steps_each, double* ms4) {
+  // Layouts: rows of 256 x 1, 128 x 2, 64 x 4, 32 x 8 cells (times the cells per thread), and the
+  // packed layout (log2_tx 5, ty 0). ms (may be NULL) receives up to n of the five times.
+  int autotune(int steps_each, double* ms, int n) {
     VB_CUDA(cudaSetDevice(device));
-    const int shapes[4][2] = {{8, 1}, {7, 2}, {6, 4}, {5, 8}};
+    const int shapes[5][2] = {{8, 1}, {7, 2}, {6, 4}, {5, 8}, {5, 0}};
     double best = 1e300;
     int bi = 0;
     P.dry = 1;
-    for (int c = 0; c < 4; ++c) {
+    for (int c = 0; c < 5; ++c) {
       log2_tx = shapes[c][0];
       ty = shapes[c][1];
       int rc = build_lists(false);
@@ -294,10 +304,10 @@ struct vl_batch {
       }
       VB_CUDA(cudaEventRecord(ev1, stream));
       VB_CUDA(cudaEventSynchronize(ev1));
-      float ms = 0.f;
-      VB_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
-      if (ms4) ms4[c] = ms / steps_each;
-      if (ms < best) { best = ms; bi = c; }
+      float t = 0.f;
+      VB_CUDA(cudaEventElapsedTime(&t, ev0, ev1));
+      if (ms && c < n) ms[c] = t / steps_each;
+      if (t < best) { best = t; bi = c; }
     }
     P.dry = 0;
     own_ok = false;  // the dry staged steps left the copy of `b`, not of `a`
@@ -547,8 +557,9 @@ int vl_batch_tunnel_info(const vl_batch* b, int k, size_t* nx, size_t* ny, size_
 
 int vl_batch_set_tile(vl_batch* b, int log2_tx, int ty) {
   if (!b || !b->built) return fail(VL_EINVAL, "batch not built");
-  if (log2_tx < 5 || log2_tx > 8 || ty < 1 || (ty << log2_tx) != vl::kBlock)
-    return fail(VL_EINVAL, "tile must be 2^log2_tx x ty = 256 cells with 32 <= 2^log2_tx <= 256");
+  const bool packed = log2_tx == 5 && ty == 0;
+  if (!packed && (log2_tx < 5 || log2_tx > 8 || ty < 1 || (ty << log2_tx) != vl::kBlock))
+    return fail(VL_EINVAL, "tile must be 2^log2_tx x ty = 256 cells with 32 <= 2^log2_tx <= 256, or (5, 0) packed");
   b->log2_tx = log2_tx;
   b->ty = ty;
   return b->build_lists(false);
@@ -593,7 +604,12 @@ int vl_batch_set_schedule(vl_batch* b, int schedule) {
 
 int vl_batch_autotune(vl_batch* b, int steps_each, double* ms4) {
   if (!b || !b->built || steps_each < 1) return fail(VL_EINVAL, "autotune: bad arguments");
-  return b->autotune(steps_each, ms4);
+  return b->autotune(steps_each, ms4, 4);
+}
+
+int vl_batch_autotune_layouts(vl_batch* b, int steps_each, double* ms, int n) {
+  if (!b || !b->built || steps_each < 1 || n < 0) return fail(VL_EINVAL, "autotune: bad arguments");
+  return b->autotune(steps_each, ms, n);
 }
 
 int vl_batch_run(vl_batch* b, uint64_t max_steps) {

@@ -4,14 +4,16 @@
 // All tunnels live in one arena: each tunnel's nine population planes are contiguous at its own
 // offset in the two population buffers, its cells at its own offset in the flag array, and its
 // boundary nodes, links and outlet nodes are concatenated into shared tables (link indices are
-// global; cell indices stay local to the tunnel). A bulk work item is a tile of a tunnel (2^log2_tx
-// cells x ty rows); a link work item is a chunk of up to kBlock boundary nodes of a tunnel. The
-// last chunk of a tunnel to finish a step runs that tunnel's epilogue (force reduction in the same
-// fixed order as a single sim, force record, t + 1). The per-node arithmetic is the single-sim
-// code (pull, link_node, collide), so in FP64 (compiled without multiply-add contraction) a tunnel
-// in a batch is bit-identical to the same tunnel run alone; the FP32 / FP16 kernels are compiled
-// with contraction, which may fuse differently here and in the single-sim kernels (last-bit
-// differences).
+// global; cell indices stay local to the tunnel). A bulk work item is a tile of a tunnel: either
+// 2^log2_tx cells (times the cells per thread) x ty rows, or, in the packed layout, 8 consecutive
+// warp segments (32 x cells-per-thread cells of a row each) in the row-major segment order of the
+// tunnel, so a tile may end in one row and go on in the next and only the last segment of each row
+// can be partly past the row end. A link work item is a chunk of up to kBlock boundary nodes of a
+// tunnel. The last chunk of a tunnel to finish a step runs that tunnel's epilogue (force reduction
+// in the same fixed order as a single sim, force record, t + 1). The per-node arithmetic is the
+// single-sim code (pull, link_node, collide), so a tunnel in a batch is bit-identical to the same
+// tunnel run alone (FP64: the reference's operation order, no contraction; the narrow formats: the
+// explicitly rounded FP32 operators every narrow kernel shares).
 //
 // The staged pairing works as for a single sim: k_batch_links<S, 1> evaluates the link rules of
 // every chunk into the per-link array, then k_batch_bulk<S, 1> updates every fluid cell of its
@@ -56,8 +58,9 @@ struct BatchState {
 struct BatchParams {
   const BatchTunnel* tun;
   BatchState* st;
-  const int4* tiles;            // (tunnel, y0, x0, -)
+  const int4* tiles;            // (tunnel, y0, x0, -); packed layout: (tunnel, first segment, 0, -)
   int log2_tx, ty;
+  int packed;                   // tiles are 8 consecutive warp segments of a tunnel
   const int4* chunks;           // (tunnel, first boundary node, count, global chunk index)
   const uint8_t* flag;
   const int32_t* bnode_idx;     // cell index local to the tunnel
@@ -86,19 +89,32 @@ struct BatchParams {
   int prefetch_tiles;           // a bulk block prefetches into the L2 the tile this far ahead (0: none)
 };
 
-// Threads of a bulk block ask the L2 for the rows of tile `k` of the list (one plane row each).
+// Packed layout: row and first cell of warp segment `w` of tile `td` (segments of `seg` cells;
+// a row holds ceil(nx / seg) of them). Past the tunnel's last segment y comes out >= ny.
+__device__ __forceinline__ void packed_seg(const int4& td, int nx, int seg, int w, int& y, int& x0) {
+  const int nseg = (nx + seg - 1) / seg;
+  const int g = td.y + w;
+  y = g / nseg;
+  x0 = (g - y * nseg) * seg;
+}
+
+// Threads of a bulk block ask the L2 for the rows of tile `k` of the list (one plane row each);
+// `width`: the tile's width in cells, or in the packed layout the segment's.
 template <class S>
 __device__ __forceinline__ void batch_prefetch(const BatchParams& p, const S* A, int k, int width) {
-  if (k >= p.ntiles || (int)threadIdx.x >= 9 * p.ty) return;
+  const int rows = p.packed ? kBlock / 32 : p.ty;
+  if (k >= p.ntiles || (int)threadIdx.x >= 9 * rows) return;
   const int4 td = __ldg(p.tiles + k);
   const BatchTunnel& T = p.tun[td.x];
-  const int i = (int)threadIdx.x % 9, y = td.y + (int)threadIdx.x / 9;
+  const int i = (int)threadIdx.x % 9, j = (int)threadIdx.x / 9;
+  int y = td.y + j, x0 = td.z;
+  if (p.packed) packed_seg(td, T.nx, width, j, y, x0);
   if (y >= T.ny) return;
   const int ym = y == 0 ? T.ny - 1 : y - 1, yp = y == T.ny - 1 ? 0 : y + 1;
   const int r = (i == 2 || i == 5 || i == 6) ? ym : ((i == 4 || i == 7 || i == 8) ? yp : y);
-  const int end = min(td.z + width, T.nx);
-  if (end <= td.z) return;
-  prefetch_l2(A + T.pop_off + (size_t)i * T.ns + (size_t)r * T.nx + td.z, (size_t)(end - td.z) * sizeof(S));
+  const int end = min(x0 + width, T.nx);
+  if (end <= x0) return;
+  prefetch_l2(A + T.pop_off + (size_t)i * T.ns + (size_t)r * T.nx + x0, (size_t)(end - x0) * sizeof(S));
 }
 
 // Controls of a tunnel at its step t (src/cases/channel.rs:118-130).
@@ -123,12 +139,18 @@ __global__ void __launch_bounds__(kBlock) k_batch_bulk(const __grid_constant__ B
   // Only tunnels that are active for the whole launch are in the tile list (the host rebuilds it
   // when a tunnel finishes), so the tile never checks the tunnel's t, which the link kernel's
   // epilogue may advance concurrently.
-  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 1 << p.log2_tx);
+  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, p.packed ? 32 : 1 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);
   const BatchTunnel& T = p.tun[td.x];
   const int nx = T.nx, ny = T.ny;
-  const int x = td.z + (int)(threadIdx.x & ((1u << p.log2_tx) - 1u));
-  const int y = td.y + (int)(threadIdx.x >> p.log2_tx);
+  int x, y;
+  if (p.packed) {
+    packed_seg(td, nx, 32, (int)(threadIdx.x >> 5), y, x);
+    x += (int)(threadIdx.x & 31u);
+  } else {
+    x = td.z + (int)(threadIdx.x & ((1u << p.log2_tx) - 1u));
+    y = td.y + (int)(threadIdx.x >> p.log2_tx);
+  }
   const bool in = x < nx && y < ny;
   if (!STAGED && !in) return;
   const S* a = A + T.pop_off;
@@ -183,14 +205,18 @@ constexpr int batch_pair_min_blocks() {
 template <class S, int STAGED>
 __global__ void __launch_bounds__(kBlock, batch_pair_min_blocks<S>()) k_batch_bulk2(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
-  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, 2 << p.log2_tx);
+  if (p.prefetch_tiles) batch_prefetch(p, A, (int)blockIdx.x + p.prefetch_tiles, p.packed ? 64 : 2 << p.log2_tx);
   const int4 td = __ldg(p.tiles + blockIdx.x);
   const BatchTunnel& T = p.tun[td.x];
   PairTask t;
   t.nx = T.nx;
   t.ny = T.ny;
-  t.y = td.y + (int)(threadIdx.x >> p.log2_tx);
-  t.xw = td.z + 2 * (int)((threadIdx.x & ((1u << p.log2_tx) - 1u)) & ~31u);
+  if (p.packed) {
+    packed_seg(td, t.nx, 64, (int)(threadIdx.x >> 5), t.y, t.xw);
+  } else {
+    t.y = td.y + (int)(threadIdx.x >> p.log2_tx);
+    t.xw = td.z + 2 * (int)((threadIdx.x & ((1u << p.log2_tx) - 1u)) & ~31u);
+  }
   if (t.y >= t.ny || t.xw >= t.nx) return;   // uniform over the warp
   t.ns = T.ns;
   t.flag = p.flag + T.cell_off;
