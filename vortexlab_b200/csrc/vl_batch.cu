@@ -38,6 +38,10 @@ int cuda_fail(cudaError_t e, const char* what) {
 
 constexpr int kGraphSteps = 32;
 
+// A tunnel's new end, set on the stream behind the steps already enqueued (the value travels as
+// a launch argument, so the host does not wait for those steps as a pageable copy would).
+__global__ void k_set_steps(vl::BatchTunnel* tun, int k, unsigned long long steps) { tun[k].steps = steps; }
+
 template <class T>
 int upload(T** dst, const std::vector<T>& v) {
   const size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
@@ -745,9 +749,11 @@ int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps) {
   if (steps > b->steps[k]) return fail(VL_EINVAL, "a tunnel cannot run longer than the steps it was added with");
   if (steps == T.steps) return VL_OK;
   T.steps = steps;
-  // ordered after a run in flight, which still reads the old end (the host value is staged
-  // before the call returns)
-  VB_CUDA(cudaMemcpyAsync(&b->d_tun[k].steps, &T.steps, sizeof T.steps, cudaMemcpyHostToDevice, b->stream));
+  // ordered after a run in flight, which still reads the old end
+  VB_CUDA(cudaSetDevice(b->device));
+  k_set_steps<<<1, 1, 0, b->stream>>>(b->d_tun, k, (unsigned long long)steps);
+  VB_CUDA(cudaGetLastError());
+  b->launches += 1;
   if (b->gexec) {       // the captured steps may cover the new end: capture again
     cudaGraphExecDestroy(b->gexec);
     b->gexec = nullptr;
