@@ -67,7 +67,7 @@ def test_batch_autotune_and_partial_runs_do_not_change_results(gpu):
             b.schedule = "staged"
         if mode.endswith("tuned"):
             ms = b.autotune(2)
-            assert set(ms) == {"256x1", "128x2", "64x4", "32x8"}
+            assert set(ms) == {"256x1", "128x2", "64x4", "32x8", "packed"}
             b.run(37)      # stop in the middle of a segment, then continue
             b.run()
         else:
