@@ -99,12 +99,14 @@ struct vl_batch {
   bool in_flight = false;                // a run was enqueued and not yet waited for
   uint64_t s_done = 0;                   // global steps complete on the device at the last wait
   cudaStream_t copy = nullptr;           // history reads beside a run in flight
+  std::vector<cudaGraphExec_t> retired;  // graphs replaced while a run may still execute them
   double* h_stage = nullptr;             // pinned staging of those reads
   size_t h_stage_cap = 0;                // doubles
 
   ~vl_batch() {
     cudaSetDevice(device);
     if (gexec) cudaGraphExecDestroy(gexec);
+    for (cudaGraphExec_t g : retired) cudaGraphExecDestroy(g);
     void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_sched,
                     d_tun, d_st, d_tiles, d_chunks, d_partials, d_hist, d_bdesc, d_segb, d_lb, d_ownc};
     for (void* p : ptrs)
@@ -121,6 +123,18 @@ struct vl_batch {
   const void* a() const { return buf[s & 1]; }
   void* b() const { return buf[(s & 1) ^ 1]; }
   void* tunnel_ptr(void* base, int k) const { return (char*)base + tun[k].pop_off * L->elem; }
+
+  // Drops the captured graph (its steps no longer fit the work lists or the tunnels' ends). A run
+  // in flight may still be executing it, and destroying it then waits for that run, so it is
+  // destroyed at the next wait instead.
+  void drop_graph() {
+    if (!gexec) return;
+    if (in_flight)
+      retired.push_back(gexec);
+    else
+      cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+  }
 
   // Work lists of the tunnels active at global step s (the ones with steps left).
   int build_lists(bool all) {
@@ -164,10 +178,7 @@ struct vl_batch {
     P.log2_tx = log2_tx;
     P.ty = ty;
     P.packed = ty == 0;
-    if (gexec) {
-      cudaGraphExecDestroy(gexec);
-      gexec = nullptr;
-    }
+    drop_graph();
     return VL_OK;
   }
 
@@ -242,6 +253,7 @@ struct vl_batch {
     for (auto& T : tun) end_all = std::max<uint64_t>(end_all, T.steps);
     const uint64_t stop = max_steps ? std::min<uint64_t>(end_all, s + max_steps) : end_all;
     VB_CUDA(cudaEventRecord(ev0, stream));
+    in_flight = true;   // from here on a graph launched below may be executing
     while (s < stop) {
       uint64_t seg_end = stop;
       for (auto& T : tun)
@@ -277,6 +289,8 @@ struct vl_batch {
     if (in_flight) timed = true;
     in_flight = false;
     s_done = s;
+    for (cudaGraphExec_t g : retired) cudaGraphExecDestroy(g);
+    retired.clear();
     return VL_OK;
   }
 
@@ -582,10 +596,7 @@ int vl_batch_set_prefetch_tiles(vl_batch* b, int tiles) {
   if (!b || !b->built || tiles < 0) return fail(VL_EINVAL, "bad arguments");
   if (tiles == b->P.prefetch_tiles) return VL_OK;
   b->P.prefetch_tiles = tiles;
-  if (b->gexec) {
-    cudaGraphExecDestroy(b->gexec);
-    b->gexec = nullptr;
-  }
+  b->drop_graph();
   return VL_OK;
 }
 
@@ -599,10 +610,7 @@ int vl_batch_get_tile(const vl_batch* b, int* log2_tx, int* ty) {
 int vl_batch_set_schedule(vl_batch* b, int schedule) {
   if (!b || schedule < 0 || schedule >= VL_SCHEDULE_COUNT) return fail(VL_EINVAL, "schedule must be 0, 1, 2 or 3");
   b->schedule = schedule;
-  if (b->gexec) {
-    cudaGraphExecDestroy(b->gexec);
-    b->gexec = nullptr;
-  }
+  b->drop_graph();
   return VL_OK;
 }
 
@@ -754,10 +762,7 @@ int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps) {
   k_set_steps<<<1, 1, 0, b->stream>>>(b->d_tun, k, (unsigned long long)steps);
   VB_CUDA(cudaGetLastError());
   b->launches += 1;
-  if (b->gexec) {       // the captured steps may cover the new end: capture again
-    cudaGraphExecDestroy(b->gexec);
-    b->gexec = nullptr;
-  }
+  b->drop_graph();      // the captured steps may cover the new end: capture again
   return VL_OK;
 }
 
