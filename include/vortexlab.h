@@ -334,7 +334,7 @@ int vl_batch_run_async(vl_batch* b, uint64_t max_steps);
 int vl_batch_wait(vl_batch* b);
 /* Force records (fx, fy per step) of n ranges, concatenated into out (2 * sum(counts) doubles):
  * steps [firsts[i], firsts[i] + counts[i]) of tunnel ks[i]. Every range must lie within the
- * tunnel's history and before the global step complete at the last wait (records a tunnel has
+ * tunnel's history and before the tunnel's steps complete at the last wait (records a tunnel has
  * not written, after it ended, are not defined). Read on a stream of its own, so it does not wait
  * for a run in flight. No reference counterpart (the on-line stopping rule's input). */
 int vl_batch_history_copy(vl_batch* b, int n, const int* ks, const uint64_t* firsts, const uint64_t* counts,
@@ -356,6 +356,14 @@ int vl_batch_download(vl_batch* b, int k, double* out);
  * the steps of a run in flight, which the change follows on the stream. Lets a caller stop each
  * tunnel at a moment it picks from the tunnel's own force history. */
 int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps);
+/* Holds tunnel k at its start state (before the batch's first step): it takes no steps until
+ * vl_batch_start. vl_batch_start starts a held tunnel: its step 0 is the batch's next global step
+ * after the steps already enqueued (start receives that global step; may be NULL). A tunnel's
+ * steps, history and vl_batch_set_steps count from its own step 0. A caller keeps a uniform-start
+ * twin of a warm-started tunnel held in the same batch and starts it only if the warm start fails
+ * (the fallback of the learned warm start). No reference counterpart. */
+int vl_batch_hold(vl_batch* b, int k);
+int vl_batch_start(vl_batch* b, int k, uint64_t* start);
 /* Density and velocity of every cell of tunnel k at its current step (solids (1, 0, 0)), FP64,
  * row-major n = nx * ny values each: Sim::macros (src/sim.rs:527-536) over the whole grid. */
 int vl_batch_macros_field(vl_batch* b, int k, double* rho, double* ux, double* uy);

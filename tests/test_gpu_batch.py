@@ -199,6 +199,46 @@ def test_async_runs_and_history_copy(gpu):
     ref.close()
 
 
+def test_held_tunnel_started_later_runs_as_from_step_zero(gpu):
+    """A tunnel held at its start state and started mid-run (vl_batch_hold / vl_batch_start) takes
+    the same steps as from global step 0: state and force history bit-identical; its steps, ends
+    and history ranges count from its own step 0; the other tunnels are untouched."""
+    V = gpu
+    from vortexlab_b200.batch import Batch
+    cases = _cases(V)
+    ref = Batch("f32")
+    for k, c in enumerate(cases):
+        ref.add(c.tunnel.spec(c.body), 50 if k == 1 else c.steps)
+    ref.build()
+    ref.run()
+    b = Batch("f32")
+    for c in cases:
+        b.add(c.tunnel.spec(c.body), c.steps)
+    b.build()
+    b.hold(1)
+    b.run_async(37)
+    b.wait()
+    assert b.status(1)[0] == 0
+    b.run_async(11)                     # global steps 37..48 in flight
+    assert b.start(1) == 48             # its step 0 follows them
+    b.set_steps(1, 50)                  # 50 of its own steps
+    with pytest.raises(V.VortexError):
+        b.start(1)                      # not held any more
+    with pytest.raises(V.VortexError):
+        b.history_copy([(1, 0, 1)])     # none of its steps is complete yet
+    b.run_async(30)
+    b.wait()
+    got = b.history_copy([(1, 0, 30)])[0]
+    b.run()
+    assert b.status(1)[0] == 50
+    assert np.array_equal(got, ref.force_history(1)[:30])
+    for k in range(len(cases)):
+        assert b.state_hash(k) == ref.state_hash(k), k
+        assert np.array_equal(b.force_history(k), ref.force_history(k)), k
+    b.close()
+    ref.close()
+
+
 def test_batch_init_from_a_grid_matches_the_host_decode(gpu):
     """vl_batch_init_grid (bilinear sampling and decoding of a coarse grid of normalised fields on
     the device) gives the fields of the host decode followed by vl_batch_init."""

@@ -79,22 +79,29 @@ def test_cached_window_stops_like_the_full_rule():
 
 class _FakeBatch:
     """Host stand-in for a batch of tunnels with the asynchronous run semantics of the library:
-    run_async advances the global step at once, records become readable after wait, and a tunnel
-    can be ended only at or after the step the enqueued run ends at."""
+    run_async advances the global step at once, records become readable after wait, a tunnel can
+    be ended only at or after the step the enqueued run ends at, and a held tunnel takes its step 0
+    at the global step after the enqueued ones when it is started."""
 
-    def __init__(self, histories, steps):
-        self.h = histories          # per tunnel (n, 2) force records
+    def __init__(self, histories, steps, held=()):
+        self.h = histories          # per tunnel (n, 2) force records of its own steps
         self.steps = list(steps)
+        self.start_at = [None if k in held else 0 for k in range(len(steps))]
         self.s = 0
         self.s_done = 0
         self.run_steps = 0
+
+    def own(self, k, g):
+        st = self.start_at[k]
+        return 0 if st is None else max(0, min(g - st, self.steps[k]))
 
     def info(self, k):
         return {"steps": self.steps[k]}
 
     def run_async(self, n):
-        end = min(max(self.steps), self.s + n)
-        self.run_steps += sum(max(0, min(e, end) - min(e, self.s)) for e in self.steps)
+        ends = [st + e for st, e in zip(self.start_at, self.steps) if st is not None]
+        end = min(max(ends), self.s + n)
+        self.run_steps += sum(self.own(k, max(end, self.s)) - self.own(k, self.s) for k in range(len(self.steps)))
         self.s = max(self.s, end)
 
     def wait(self):
@@ -106,16 +113,21 @@ class _FakeBatch:
     def history_copy(self, ranges):
         out = []
         for k, first, count in ranges:
-            assert first + count <= min(self.s_done, self.steps[k]), (k, first, count, self.s_done)
+            assert first + count <= self.own(k, self.s_done), (k, first, count, self.s_done)
             out.append(self.h[k][first:first + count])
         return out
 
     def set_steps(self, k, steps):
-        assert steps >= self.s and steps <= self.steps[k]
+        assert steps >= self.own(k, self.s) and steps <= self.steps[k]
         self.steps[k] = steps
 
+    def start(self, k):
+        assert self.start_at[k] is None
+        self.start_at[k] = self.s
+        return self.s
+
     def status(self, k):
-        return min(self.s, self.steps[k]), False, None
+        return self.own(k, self.s), False, None
 
 
 class _Tun:
@@ -161,4 +173,29 @@ def test_overlapped_batch_checks_stop_each_tunnel_within_a_chunk():
         else:
             assert r["stop"]["steps"] == want, (k, r["stop"], want)
             assert want <= r["steps"] <= want + chunk, (k, r["steps"], want)
+    assert b.run_steps == sum(r["steps"] for r in res)
+
+
+def test_overlapped_checks_start_a_held_twin_when_a_tunnel_fails():
+    """A tunnel that reaches its end unsettled starts its held twin at once; the twin is checked
+    from its own step 0 and stops where the rule first holds on its own records; a twin of a
+    settled tunnel is never started."""
+    from vortexlab_b200.online import batch_online
+    rule = StopRule()
+    k_force = 2.0 / (0.05 * 0.05 * 20.0)
+    spu = 300
+    hist = []
+    for st in (400.0, 10.0, 10.0, 400.0):         # 0 never settles, 2 is its twin and settles; 1 settles, 3 its twin
+        cd, cl, dt = _history(units=60.0, dt=1.0 / spu, settle=st)
+        hist.append(np.stack([cd / k_force, cl / k_force], axis=1))
+    cases = [_Case(spu) for _ in hist]
+    b = _FakeBatch(hist, [len(h) for h in hist], held=(2, 3))
+    res, _ = batch_online(b, cases, rule, max_units=60.0, check_units=2.0, twins={0: 2, 1: 3})
+    assert res[0]["stop"] is None and res[0]["steps"] == len(hist[0])
+    assert res[2]["start"] is not None and res[2]["start"] >= len(hist[0])
+    assert res[2]["stop"] is not None
+    assert res[1]["stop"] is not None and res[3]["start"] is None and res[3]["steps"] == 0
+    cd, cl = hist[2][:, 0] * k_force, hist[2][:, 1] * k_force
+    want = next(e for e in range(2 * spu, len(cd) + 1, 2 * spu) if settled(cd[:e], cl[:e], 1.0 / spu, rule) is not None)
+    assert abs(res[2]["stop"]["steps"] - want) <= 2 * spu      # its checks fall between the 2-unit marks
     assert b.run_steps == sum(r["steps"] for r in res)

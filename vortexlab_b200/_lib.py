@@ -136,6 +136,8 @@ def _declare(L):
         "vl_batch_wait": (i, [vp]),
         "vl_batch_history_copy": (i, [vp, i, P(i), P(u64), P(u64), P(d)]),
         "vl_batch_autotune_layouts": (i, [vp, i, P(d), i]),
+        "vl_batch_hold": (i, [vp, i]),
+        "vl_batch_start": (i, [vp, i, P(u64)]),
         "vl_batch_set_prefetch_tiles": (i, [vp, i]),
         "vl_batch_set_cells_per_thread": (i, [vp, i]),
         "vl_batch_set_tile": (i, [vp, i, i]),

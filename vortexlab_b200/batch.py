@@ -113,6 +113,16 @@ class Batch:
     def wait(self):
         check(lib.vl_batch_wait(self._h))
 
+    def hold(self, k):
+        """Keeps tunnel k at its start state, taking no steps, until `start(k)` (before the first step)."""
+        check(lib.vl_batch_hold(self._h, k))
+
+    def start(self, k) -> int:
+        """Starts held tunnel k at the next global step after the enqueued ones; returns that step."""
+        out = C.c_uint64()
+        check(lib.vl_batch_start(self._h, k, C.byref(out)))
+        return out.value
+
     def history_copy(self, ranges):
         """Force records of several tunnels at once: `ranges` is a list of (k, first, count) with
         every step complete at the last `wait`; returns one (count, 2) array per range. Does not

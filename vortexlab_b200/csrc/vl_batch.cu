@@ -61,6 +61,10 @@ struct vl_batch {
   std::vector<uint64_t> steps;
   bool built = false;
   std::vector<vl::BatchTunnel> tun;
+  // Global step at which each tunnel takes its step 0 (kHeld: not started yet). A tunnel is active
+  // at global step s while start <= s < start + its steps; the device counts in tunnel steps.
+  static constexpr uint64_t kHeld = ~0ull;
+  std::vector<uint64_t> start;
   std::vector<int4> chunks_all;          // every chunk, tunnel-major
   std::vector<int> chunk_first;          // first chunk of each tunnel in chunks_all
   void* buf[2] = {nullptr, nullptr};
@@ -123,6 +127,12 @@ struct vl_batch {
   const void* a() const { return buf[s & 1]; }
   void* b() const { return buf[(s & 1) ^ 1]; }
   void* tunnel_ptr(void* base, int k) const { return (char*)base + tun[k].pop_off * L->elem; }
+  // Global step after the last step of tunnel k (0 while it is held).
+  uint64_t end_of(size_t k) const { return start[k] == kHeld ? 0 : start[k] + tun[k].steps; }
+  // Steps tunnel k has done (or has enqueued) by global step g.
+  uint64_t done_by(size_t k, uint64_t g) const {
+    return start[k] == kHeld || g <= start[k] ? 0 : std::min<uint64_t>(g - start[k], tun[k].steps);
+  }
 
   // Drops the captured graph (its steps no longer fit the work lists or the tunnels' ends). A run
   // in flight may still be executing it, and destroying it then waits for that run, so it is
@@ -144,7 +154,7 @@ struct vl_batch {
     const int seg = 32 << (P.pairs ? 1 : 0);               // packed layout: cells per warp segment
     const int wpb = vl::kBlock / 32;                       // warp segments per packed tile
     for (size_t k = 0; k < tun.size(); ++k) {
-      if (!all && s >= tun[k].steps) continue;
+      if (!all && s >= end_of(k)) continue;
       const vl::BatchTunnel& T = tun[k];
       if (ty == 0) {
         const int total = T.ny * ((T.nx + seg - 1) / seg);
@@ -166,7 +176,7 @@ struct vl_batch {
     // copies are ordered after any run still in flight on the stream, which reads the old lists.
     VB_CUDA(cudaMemcpyAsync(d_chunks, chunks_h.data(), chunks_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
     listed.assign(tun.size(), 0);
-    for (size_t k = 0; k < tun.size(); ++k) listed[k] = all || s < tun[k].steps;
+    for (size_t k = 0; k < tun.size(); ++k) listed[k] = all || s < end_of(k);
     listed_tx = log2_tx;
     listed_ty = ty;
     listed_pairs = P.pairs;
@@ -186,7 +196,7 @@ struct vl_batch {
   bool lists_current() const {
     if (listed.size() != tun.size() || listed_tx != log2_tx || listed_ty != ty || listed_pairs != P.pairs) return false;
     for (size_t k = 0; k < tun.size(); ++k)
-      if ((bool)listed[k] != (s < tun[k].steps)) return false;
+      if ((bool)listed[k] != (s < end_of(k))) return false;
     return true;
   }
 
@@ -250,14 +260,14 @@ struct vl_batch {
   int enqueue_run(uint64_t max_steps) {
     VB_CUDA(cudaSetDevice(device));
     uint64_t end_all = 0;
-    for (auto& T : tun) end_all = std::max<uint64_t>(end_all, T.steps);
+    for (size_t k = 0; k < tun.size(); ++k) end_all = std::max<uint64_t>(end_all, end_of(k));
     const uint64_t stop = max_steps ? std::min<uint64_t>(end_all, s + max_steps) : end_all;
     VB_CUDA(cudaEventRecord(ev0, stream));
     in_flight = true;   // from here on a graph launched below may be executing
     while (s < stop) {
       uint64_t seg_end = stop;
-      for (auto& T : tun)
-        if (T.steps > s) seg_end = std::min<uint64_t>(seg_end, T.steps);
+      for (size_t k = 0; k < tun.size(); ++k)
+        if (end_of(k) > s) seg_end = std::min<uint64_t>(seg_end, end_of(k));
       int rc = lists_current() ? VL_OK : build_lists(false);
       if (rc) return rc;
       if ((rc = prepare_steps())) return rc;
@@ -553,6 +563,7 @@ int vl_batch_build(vl_batch* b) {
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     P.prefetch_tiles = 3 * sms;
   }
+  b->start.assign(nt, 0);
   b->built = true;
   // The host plans (domains) are no longer needed on the host except their sizes.
   for (auto& pl : b->plans) {
@@ -647,7 +658,8 @@ int vl_batch_history_copy(vl_batch* b, int n, const int* ks, const uint64_t* fir
     if (k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "tunnel index out of range");
     if (firsts[i] > b->steps[k] || counts[i] > b->steps[k] - firsts[i])
       return fail(VL_EINVAL, "range past the tunnel's force history");
-    if (firsts[i] + counts[i] > b->s_done) return fail(VL_EINVAL, "range past the steps complete at the last wait");
+    if (firsts[i] + counts[i] > b->done_by(k, b->s_done))
+      return fail(VL_EINVAL, "range past the steps complete at the last wait");
   }
   VB_CUDA(cudaSetDevice(b->device));
   size_t total = 0;
@@ -750,10 +762,31 @@ int vl_batch_download(vl_batch* b, int k, double* out) {
   return VL_OK;
 }
 
+int vl_batch_hold(vl_batch* b, int k) {
+  if (!b || !b->built || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  if (b->s != 0) return fail(VL_EINVAL, "a tunnel can only be held before the batch's first step");
+  if (b->start[k] == vl_batch::kHeld) return VL_OK;
+  b->start[k] = vl_batch::kHeld;
+  b->drop_graph();
+  return VL_OK;
+}
+
+int vl_batch_start(vl_batch* b, int k, uint64_t* start) {
+  if (!b || !b->built || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
+  if (b->start[k] != vl_batch::kHeld) return fail(VL_EINVAL, "the tunnel is not held");
+  b->start[k] = b->s;        // its step 0 follows the steps already enqueued
+  b->own_ok = false;         // the staged step's copy of boundary populations lacks it
+  b->drop_graph();
+  if (start) *start = b->s;
+  return VL_OK;
+}
+
 int vl_batch_set_steps(vl_batch* b, int k, uint64_t steps) {
   if (!b || !b->built || k < 0 || (size_t)k >= b->tun.size()) return fail(VL_EINVAL, "bad arguments");
   vl::BatchTunnel& T = b->tun[k];
-  if (steps < b->s || b->s > T.steps) return fail(VL_EINVAL, "the tunnel has already run past that step");
+  const uint64_t done = b->done_by(k, b->s);
+  if (steps < done || (b->start[k] != vl_batch::kHeld && b->s > b->end_of(k)))
+    return fail(VL_EINVAL, "the tunnel has already run past that step");
   if (steps > b->steps[k]) return fail(VL_EINVAL, "a tunnel cannot run longer than the steps it was added with");
   if (steps == T.steps) return VL_OK;
   T.steps = steps;

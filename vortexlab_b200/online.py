@@ -36,6 +36,11 @@ import numpy as np
 from . import signal
 
 
+# Global steps per chunk of a batch run = the most frequent tunnel's check interval / CHUNK_DIV:
+# a tunnel found settled runs on to the end of the chunk already enqueued.
+CHUNK_DIV = 2
+
+
 @dataclass
 class StopRule:
     tol: float = 0.002          # agreement of the trailing windows (relative, c_D mean and St)
@@ -162,40 +167,60 @@ def plain_arm(cases, rule: StopRule, max_units=100.0, check_units=2.0, log=None)
     return out
 
 
-def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chunk_global=None):
-    """Runs a built batch (every tunnel added with max_units of steps, all starting at step 0) and
+def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chunk_global=None, twins=None):
+    """Runs a built batch (`cases[i]` describes its tunnel i, added with max_units of steps) and
     stops each tunnel when the rule holds on its own history. The device runs the next chunk of
     global steps while the host reads the records of the chunk just finished (one copy for every
-    tunnel due a check) and applies the rule, so a tunnel found settled at step t is ended at the
-    end of the chunk already enqueued: it runs at most one chunk past its stop, and those steps
-    count in the wall time and in the lattice updates like any other. A running tunnel's step is
-    the batch's global step; a non-finite force record marks it diverged (and ends it). Returns
-    per-tunnel dicts (stop or None, steps run, finite) and the host seconds spent in the checks
-    (overlapped with the device)."""
+    tunnel due a check) and applies the rule, so a tunnel found settled at its step t is ended at
+    the end of the chunk already enqueued: it runs at most one chunk past its stop, and those steps
+    count in the wall time and in the lattice updates like any other. A non-finite force record
+    marks a tunnel diverged (and ends it). `twins` maps a tunnel to a held tunnel of the same batch
+    (vl_batch_hold): when the tunnel diverges or reaches its end unsettled, its twin is started at
+    once (vl_batch_start), beside the tunnels still running, and checked like any other from its
+    own step 0. Returns per-tunnel dicts (stop or None, steps run, finite, start: the global step of
+    its step 0 or None if never started) and the host seconds spent in the checks (overlapped with
+    the device)."""
     nt = len(cases)
+    twins = dict(twins or {})
+    held = set(twins.values())
     spu = np.array([c.tunnel.steps_per_unit() for c in cases])
     dt = 1.0 / spu
     every = np.maximum(1, (check_units * spu).astype(np.int64))   # steps between a tunnel's checks
     if chunk_global is None:
-        chunk_global = int(every.min())
-    ends = [int(b.info(k)["steps"]) for k in range(nt)]
+        chunk_global = max(1, int(every.min()) // CHUNK_DIV)
+    ends = [int(b.info(k)["steps"]) for k in range(nt)]            # in the tunnel's own steps
     # c_D and c_L of each tunnel, filled in place as the records arrive
     cds = [np.empty(e) for e in ends]
     cls = [np.empty(e) for e in ends]
     have = [0] * nt
     caches = [dict() for _ in range(nt)]
     next_check = every.copy()
-    active = set(range(nt))
-    result = [dict(stop=None, steps=0, finite=True) for _ in range(nt)]
+    start = [None if k in held else 0 for k in range(nt)]
+    active = set(k for k in range(nt) if k not in held)
+    result = [dict(stop=None, steps=0, finite=True, start=start[k]) for k in range(nt)]
     host_s = 0.0
     parts = dict(wait_s=0.0, copy_s=0.0, end_s=0.0)
 
-    def end_at(k, s_next):
-        if s_next < ends[k]:
+    def own(k, g):           # steps tunnel k has done by global step g
+        return 0 if start[k] is None else max(0, min(g - start[k], ends[k]))
+
+    def end_at(k, g_next):
+        e = g_next - start[k]
+        if e < ends[k]:
             t1 = time.perf_counter()
-            b.set_steps(k, s_next)
+            b.set_steps(k, e)
             parts["end_s"] += time.perf_counter() - t1
-            ends[k] = s_next
+            ends[k] = e
+
+    def fail_over(k):
+        j = twins.get(k)
+        if j is not None and start[j] is None:
+            start[j] = b.start(j)
+            result[j]["start"] = start[j]
+            active.add(j)
+
+    def pending(g):
+        return any(start[k] + ends[k] > g for k in active)
 
     b.run_async(int(chunk_global))
     while True:
@@ -203,14 +228,14 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
         b.wait()
         parts["wait_s"] += time.perf_counter() - t1
         s_done = b.global_step()
-        more = any(ends[k] > s_done for k in active)
+        more = pending(s_done)
         if more:
             b.run_async(int(chunk_global))
         s_next = b.global_step()
         t0 = time.perf_counter()
         due = []
         for k in sorted(active):
-            t = min(s_done, ends[k])
+            t = own(k, s_done)
             if t < next_check[k] and t < ends[k]:
                 continue
             due.append((k, have[k], t - have[k]))
@@ -230,6 +255,7 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
                 result[k]["finite"] = False
                 active.discard(k)
                 end_at(k, s_next)
+                fail_over(k)
                 continue
             r = settled(cds[k][:t], cls[k][:t], dt[k], rule, caches[k])
             if r is not None:
@@ -238,9 +264,12 @@ def batch_online(b, cases, rule: StopRule, max_units=100.0, check_units=2.0, chu
                 end_at(k, s_next)
             elif t >= ends[k]:
                 active.discard(k)
+                fail_over(k)
         host_s += time.perf_counter() - t0
         if not more:
-            break
+            if not pending(s_done):
+                break
+            b.run_async(int(chunk_global))      # twins started just now
     b.wait()
     for k in range(nt):
         t, nonfinite, _ = b.status(k)
@@ -258,53 +287,51 @@ def _lattice_cells(case):
 
 def fast_arm(cases, rule: StopRule, net=None, precision="f32", max_units=100.0, check_units=2.0):
     """All cases in one FP32 batch, uniform start (net None) or warm start from the network,
-    stopped on-line; warm tunnels that diverge or do not settle are rerun from the uniform start
-    in a fallback batch. Returns (per-case dicts, measured wall seconds, info). The wall time is
-    what the plain arm's is: the runs themselves (here the network's encoding, inference and
-    initialisation, the batch run with its on-line checks and the fallback run), not the building
-    of the domains or the autotuning, which the plain arm does untimed too."""
+    stopped on-line. With the network, each case's uniform-start twin (inlet ramp and twist) waits
+    held in the same batch and is started the moment the warm-started tunnel diverges or reaches
+    max_units unsettled: the fallback runs beside the tunnels still running and its steps are
+    counted. Returns (per-case dicts, measured wall seconds, info). The wall time is what the plain
+    arm's is: the runs themselves (here the network's encoding, inference and initialisation and
+    the batch run with its on-line checks and fallbacks), not the building of the domains or the
+    autotuning, which the plain arm does untimed too."""
     from .batch import Batch
     for c in cases:
         c.units = max_units
+    n = len(cases)
     t_init = 0.0
+    twins = None
     if net is not None:
         from .warmstart import warm_batch
-        b, t_init = warm_batch(net, cases, precision)
+        b, t_init = warm_batch(net, cases, precision, twins=True)
+        listed = list(cases) + list(cases)
+        twins = {k: n + k for k in range(n)}
     else:
         b = Batch(precision)
         for c in cases:
             b.add(c.tunnel.spec(c.body), c.steps)
         b.build()
+        listed = list(cases)
     tune = b.autotune(3)
     t_run = time.perf_counter()
-    res, host_s = batch_online(b, cases, rule, max_units, check_units)
+    res_all, host_s = batch_online(b, listed, rule, max_units, check_units, twins=twins)
     run_s = time.perf_counter() - t_run
-    lu = sum(_lattice_cells(c) * r["steps"] for c, r in zip(cases, res))
+    lu = sum(_lattice_cells(c) * r["steps"] for c, r in zip(listed, res_all))
     info = dict(tile=b.tile, autotune_ms_per_step=tune, init_s=t_init, run_s=run_s, check_host_s=host_s,
                 check_parts={k: round(v, 3) for k, v in batch_online.last_parts.items()},
                 device_ms=b.last_run_ms(), lattice_updates=lu)
     b.close()
-    for r in res:
+    res = []
+    for k in range(n):
+        r = res_all[k]
         r["fallback"] = False
-    redo = [k for k, r in enumerate(res) if net is not None and r["stop"] is None]
-    if redo:
-        fb = Batch(precision)
-        sub = [cases[k] for k in redo]
-        for c in sub:
-            fb.add(c.tunnel.spec(c.body), c.steps)
-        fb.build()
-        t_fb = time.perf_counter()
-        res_fb, host_fb = batch_online(fb, sub, rule, max_units, check_units)
-        info["fallback_s"] = time.perf_counter() - t_fb
-        info["fallback_tunnels"] = len(redo)
-        lu_fb = sum(_lattice_cells(c) * r["steps"] for c, r in zip(sub, res_fb))
-        info["lattice_updates"] += lu_fb
-        fb.close()
-        for k, r in zip(redo, res_fb):
-            r["fallback"] = True
-            r["first_steps"] = res[k]["steps"]
-            res[k] = r
-    wall = t_init + run_s + info.get("fallback_s", 0.0)
+        if twins is not None and res_all[n + k]["start"] is not None:
+            rf = res_all[n + k]
+            rf["fallback"] = True
+            rf["first_steps"] = r["steps"]
+            r = rf
+        res.append(r)
+    info["fallback_tunnels"] = sum(r["fallback"] for r in res)
+    wall = t_init + run_s
     info["wall_s"] = wall
     return res, wall, info
 

@@ -616,17 +616,25 @@ def masked_mse(pred, data: Dataset):
 
 
 # ---------------------------------------------------------------------------- warm-started runs
-def warm_batch(net, cases, precision="f32", batch=16):
+def warm_batch(net, cases, precision="f32", batch=16, twins=False):
     """A built batch of the cases in their warm form (no ramp, no twist), every tunnel initialised
     from the network's prediction: inputs encoded on the host from the tunnels' flags, the network
-    and the decode to lattice fields (vl_batch_init_grid) on the device. Returns (batch, seconds
-    spent on encoding, inference and initialisation)."""
+    and the decode to lattice fields (vl_batch_init_grid) on the device. With `twins`, tunnels
+    n .. 2n - 1 are the cases' uniform-start forms (inlet ramp and twist), held (vl_batch_hold)
+    until a caller starts one as the fallback of its warm twin. Returns (batch, seconds spent on
+    encoding, inference and initialisation)."""
     from .batch import Batch
     torch = _t()
     b = Batch(precision)
     for c in cases:
         b.add(c.tunnel.spec_warm(c.body), c.steps)
+    if twins:
+        for c in cases:
+            b.add(c.tunnel.spec(c.body), c.steps)
     b.build()
+    if twins:
+        for k in range(len(cases), 2 * len(cases)):
+            b.hold(k)
     if net.B != batch:          # the network's activation buffers: set-up, like building the batch
         net.alloc(batch)
     t0 = time.perf_counter()
