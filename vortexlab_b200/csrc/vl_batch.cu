@@ -80,6 +80,7 @@ struct vl_batch {
   int4* d_tiles = nullptr;
   size_t tiles_cap = 0;
   int4* d_chunks = nullptr;
+  int* d_outl = nullptr;                 // active tunnels with an absorbing outlet
   double* d_partials = nullptr;
   double* d_hist = nullptr;
   int2* d_bdesc = nullptr;               // staged step: per boundary node {first link, direction mask}
@@ -97,6 +98,7 @@ struct vl_batch {
   uint64_t launches = 0;
   cudaGraphExec_t gexec = nullptr;
   std::vector<int4> tiles_h, chunks_h;   // host copies of the current work lists
+  std::vector<int> outl_h;
   std::vector<char> listed;              // which tunnels the current work lists hold
   int listed_tx = -1, listed_ty = -1, listed_pairs = -1;
   bool timed = false;
@@ -112,7 +114,7 @@ struct vl_batch {
     if (gexec) cudaGraphExecDestroy(gexec);
     for (cudaGraphExec_t g : retired) cudaGraphExecDestroy(g);
     void* ptrs[] = {buf[0], buf[1], d_flag, d_bidx, d_bfirst, d_links, d_pidx, d_pn, d_sched,
-                    d_tun, d_st, d_tiles, d_chunks, d_partials, d_hist, d_bdesc, d_segb, d_lb, d_ownc};
+                    d_tun, d_st, d_tiles, d_chunks, d_outl, d_partials, d_hist, d_bdesc, d_segb, d_lb, d_ownc};
     for (void* p : ptrs)
       if (p) cudaFree(p);
     cudaEvent_t evs[] = {ev_fork, ev_join, ev0, ev1};
@@ -150,6 +152,7 @@ struct vl_batch {
   int build_lists(bool all) {
     tiles_h.clear();
     chunks_h.clear();
+    outl_h.clear();
     const int tx = (1 << log2_tx) << (P.pairs ? 1 : 0);   // cells per tile row
     const int seg = 32 << (P.pairs ? 1 : 0);               // packed layout: cells per warp segment
     const int wpb = vl::kBlock / 32;                       // warp segments per packed tile
@@ -164,6 +167,7 @@ struct vl_batch {
           for (int x0 = 0; x0 < T.nx; x0 += tx) tiles_h.push_back(make_int4((int)k, y0, x0, 0));
       }
       for (int c = 0; c < T.nchunks; ++c) chunks_h.push_back(chunks_all[chunk_first[k] + c]);
+      if (T.absorbing && T.np > 0 && T.nchunks > 0) outl_h.push_back((int)k);
     }
     if (tiles_h.size() > tiles_cap) {
       if (d_tiles) cudaFree(d_tiles);
@@ -175,6 +179,8 @@ struct vl_batch {
     // Pageable host to device: the host vectors are staged before the calls return, and the
     // copies are ordered after any run still in flight on the stream, which reads the old lists.
     VB_CUDA(cudaMemcpyAsync(d_chunks, chunks_h.data(), chunks_h.size() * sizeof(int4), cudaMemcpyHostToDevice, stream));
+    if (!outl_h.empty())
+      VB_CUDA(cudaMemcpyAsync(d_outl, outl_h.data(), outl_h.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
     listed.assign(tun.size(), 0);
     for (size_t k = 0; k < tun.size(); ++k) listed[k] = all || s < end_of(k);
     listed_tx = log2_tx;
@@ -185,12 +191,17 @@ struct vl_batch {
     P.ntiles = ntiles;
     P.tiles = d_tiles;
     P.chunks = d_chunks;
+    P.outl = d_outl;
+    P.noutl = (int)outl_h.size();
     P.log2_tx = log2_tx;
     P.ty = ty;
     P.packed = ty == 0;
     drop_graph();
     return VL_OK;
   }
+
+  // Kernels a step launches: bulk and links, and the outlet offsets where a tunnel has an outlet.
+  int per_step() const { return (ntiles > 0) + (nchunks > 0) + (nchunks > 0 && P.noutl > 0); }
 
   // Whether the work lists already hold exactly the tunnels active at step s.
   bool lists_current() const {
@@ -277,12 +288,12 @@ struct vl_batch {
           if (rc) return rc;
           VB_CUDA(cudaGraphLaunch(gexec, stream));
           s += kGraphSteps;
-          launches += 2 * kGraphSteps;
+          launches += (uint64_t)per_step() * kGraphSteps;
         } else {
           cudaError_t e = enqueue_step();
           if (e != cudaSuccess) return cuda_fail(e, "batch step");
           ++s;
-          launches += 2;
+          launches += per_step();
         }
       }
       own_ok = schedule == 3;
@@ -495,6 +506,7 @@ int vl_batch_build(vl_batch* b) {
   VB_CUDA(cudaMalloc(&b->d_lb, std::max<size_t>(links.size() * r_elem, 16)));
   VB_CUDA(cudaMalloc(&b->d_ownc, std::max<size_t>((size_t)nbs * 9 * b->L->elem, 16)));
   VB_CUDA(cudaMalloc(&b->d_chunks, std::max<size_t>(b->chunks_all.size(), 1) * sizeof(int4)));
+  VB_CUDA(cudaMalloc(&b->d_outl, std::max<size_t>(nt, 1) * sizeof(int)));
   VB_CUDA(cudaMalloc(&b->d_partials, std::max(nchunk, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaMalloc(&b->d_hist, std::max<unsigned long long>(hist, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));

@@ -51,7 +51,8 @@ struct BatchState {
   unsigned long long nonfinite_t;
   unsigned int arrive;
   int nonfinite;
-  double drho;
+  double drho;                  // the outlet offset of the last step (an observable)
+  double drho_now;              // the outlet offset of the step being taken (k_batch_outlet)
   double force[2];
 };
 
@@ -62,6 +63,8 @@ struct BatchParams {
   int log2_tx, ty;
   int packed;                   // tiles are 8 consecutive warp segments of a tunnel
   const int4* chunks;           // (tunnel, first boundary node, count, global chunk index)
+  const int* outl;              // active tunnels with an absorbing outlet
+  int noutl;
   const uint8_t* flag;
   const int32_t* bnode_idx;     // cell index local to the tunnel
   const int32_t* bnode_first;   // global link index; total_nb + 1 entries
@@ -237,11 +240,28 @@ __global__ void __launch_bounds__(kBlock, batch_pair_min_blocks<S>()) k_batch_bu
 
 // STAGED = 1: the link rules only (k_links_stage for a chunk): own populations from the compact
 // copy, the returning populations to the per-link array, no pull, collision or store.
+// The outlet density offset of each active absorbing tunnel at its current step, once per tunnel
+// (src/sim.rs:425-440; the sequential sum in outlet-node order of the reference), for every link
+// chunk of that tunnel to read; launched on the link kernel's stream just before it.
+template <class S>
+__global__ void __launch_bounds__(kBlock) k_batch_outlet(const __grid_constant__ BatchParams p, const S* __restrict__ A) {
+  __shared__ double s_un[kBlock];
+  const int k = __ldg(p.outl + blockIdx.x);
+  const BatchTunnel& T = p.tun[k];
+  BatchState* st = &p.st[k];
+  const unsigned long long t = st->t;
+  if (t >= T.steps) return;
+  double vs[4], target;
+  tunnel_controls(p, T, t, vs, target);
+  const double drho = outlet_offset(A + T.pop_off, T.ns, p.pnode_idx + T.p_off, p.pnode_n + 2 * T.p_off, T.np, 0.0,
+                                    0.0, target, p.sqrt_cs2, s_un);
+  if (threadIdx.x == 0) st->drho_now = drho;
+}
+
 template <class S, int STAGED>
 __global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ BatchParams p, const S* __restrict__ A,
                                                         S* __restrict__ B) {
   using R = typename Store<S>::R;
-  __shared__ double s_un[kBlock];
   __shared__ double s_acc[2][kBlock];
   __shared__ double red[kBlock];
   __shared__ int last;
@@ -255,10 +275,7 @@ __global__ void __launch_bounds__(kBlock) k_batch_links(const __grid_constant__ 
   S* b = B + T.pop_off;
   double vs[4], target;
   tunnel_controls(p, T, t, vs, target);
-  const double drho = (T.absorbing && T.np > 0)
-                          ? outlet_offset(a, T.ns, p.pnode_idx + T.p_off, p.pnode_n + 2 * T.p_off, T.np, 0.0, 0.0,
-                                          target, p.sqrt_cs2, s_un)
-                          : 0.0;
+  const double drho = (T.absorbing && T.np > 0) ? st->drho_now : 0.0;   // k_batch_outlet, just before
   if (cd.w == T.chunk_off && tid == 0 && !p.dry) st->drho = drho;
   s_acc[0][tid] = 0.0;
   s_acc[1][tid] = 0.0;

@@ -154,6 +154,7 @@ struct LaunchImpl {
                                 cudaStream_t s) {
     bool pairs = false;
     if constexpr (!std::is_same<S, double>::value) pairs = p.pairs != 0;
+    if ((which & 1) && nchunks > 0 && p.noutl > 0) k_batch_outlet<S><<<p.noutl, kBlock, 0, s>>>(p, (const S*)a);
     if (which & 4) {
       if ((which & 1) && nchunks > 0) k_batch_links<S, 1><<<nchunks, kBlock, 0, s>>>(p, (const S*)a, (S*)b);
       if ((which & 2) && ntiles > 0) {
