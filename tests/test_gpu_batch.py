@@ -82,8 +82,8 @@ def test_batch_autotune_and_partial_runs_do_not_change_results(gpu):
 def test_batch_init_and_macros_match_single_runs(gpu, prec):
     """A tunnel of the warm form (no ramp, no twist) initialised in a batch from given fields
     matches the same channel initialised alone with Sim::init: bit-identical in FP64; in FP32 the
-    reduced-precision kernels are compiled with multiply-add contraction, which the compiler may
-    place differently in the batched and the single-tunnel kernel, so the two agree to rounding."""
+    comparison allows rounding (the bit-identity of batched and single FP32 runs is the first test
+    of this file)."""
     V = gpu
     from vortexlab_b200 import Channel
     from vortexlab_b200.batch import Batch

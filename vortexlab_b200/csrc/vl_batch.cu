@@ -510,7 +510,15 @@ int vl_batch_build(vl_batch* b) {
   VB_CUDA(cudaMalloc(&b->d_partials, std::max(nchunk, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaMalloc(&b->d_hist, std::max<unsigned long long>(hist, 1) * 2 * sizeof(double)));
   VB_CUDA(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+#ifdef VL_BATCH_AUX_PRIORITY
+  {
+    int lo = 0, hi = 0;
+    VB_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+    VB_CUDA(cudaStreamCreateWithPriority(&b->aux, cudaStreamNonBlocking, hi));
+  }
+#else
   VB_CUDA(cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking));
+#endif
   VB_CUDA(cudaStreamCreateWithFlags(&b->copy, cudaStreamNonBlocking));
   VB_CUDA(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
   VB_CUDA(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
