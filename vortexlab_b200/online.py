@@ -17,8 +17,9 @@ The time-to-converged study (`comparison`) runs three arms on the same tunnels:
   statistics of its last window at `max_units` are the reference values.
 * cold: FP32, all tunnels in one batch, uniform start, stopped on-line.
 * warm: FP32, all tunnels in one batch in their warm form (no ramp, no twist), started from the
-  network's prediction, stopped on-line; a tunnel that diverges or has not settled by
-  `max_units` is run again from the uniform start in a fallback batch, whose time is added.
+  network's prediction, stopped on-line; each tunnel's uniform-start twin waits held in the same
+  batch and is started the moment the tunnel diverges or reaches `max_units` unsettled (the
+  fallback), its steps and time counted with the rest.
 
 Every tunnel is counted. The aggregate speed-up is measured: the plain arm's summed elapsed times
 to converged against the fast arm's whole wall time (inference, runs, on-line checks, fallback).
