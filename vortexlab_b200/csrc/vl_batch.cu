@@ -129,6 +129,9 @@ struct vl_batch {
   const void* a() const { return buf[s & 1]; }
   void* b() const { return buf[(s & 1) ^ 1]; }
   void* tunnel_ptr(void* base, int k) const { return (char*)base + tun[k].pop_off * L->elem; }
+  // The buffer that holds tunnel k's state after t of its own steps (its step 0 took the global
+  // step start; a held tunnel's start state is in both buffers).
+  int parity(size_t k, uint64_t t) const { return (int)(((start[k] == kHeld ? 0 : start[k]) + t) & 1); }
   // Global step after the last step of tunnel k (0 while it is held).
   uint64_t end_of(size_t k) const { return start[k] == kHeld ? 0 : start[k] + tun[k].steps; }
   // Steps tunnel k has done (or has enqueued) by global step g.
@@ -774,7 +777,7 @@ int vl_batch_download(vl_batch* b, int k, double* out) {
   const vl::BatchTunnel& T = b->tun[k];
   double* tmp = nullptr;
   VB_CUDA(cudaMalloc(&tmp, 9 * n * sizeof(double)));
-  cudaError_t e = b->L->to_f64((int)n, T.ns, b->tunnel_ptr(b->buf[st.t & 1], k), tmp, b->stream);
+  cudaError_t e = b->L->to_f64((int)n, T.ns, b->tunnel_ptr(b->buf[b->parity(k, st.t)], k), tmp, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, tmp, 9 * n * 8, cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   cudaFree(tmp);
@@ -829,7 +832,7 @@ int vl_batch_macros_field(vl_batch* b, int k, double* rho, double* ux, double* u
   const vl::BatchTunnel& T = b->tun[k];
   double* tmp = nullptr;
   VB_CUDA(cudaMalloc(&tmp, 3 * n * sizeof(double)));
-  cudaError_t e = b->L->macros((int)n, T.ns, b->d_flag + T.cell_off, 0.0, 0.0, b->tunnel_ptr(b->buf[st.t & 1], k), tmp,
+  cudaError_t e = b->L->macros((int)n, T.ns, b->d_flag + T.cell_off, 0.0, 0.0, b->tunnel_ptr(b->buf[b->parity(k, st.t)], k), tmp,
                                tmp + n, tmp + 2 * n, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(rho, tmp, n * 8, cudaMemcpyDeviceToHost, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(ux, tmp + n, n * 8, cudaMemcpyDeviceToHost, b->stream);
