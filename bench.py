@@ -26,7 +26,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BOX = dict(nx=8192, ny=4096, seed=0x5EED0001, fraction=0.05, tau=0.55, u=0.05)
-BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36, "f16c": 36}
+BYTES_PER_LU = {"f64": 144, "f32": 72, "f16s": 36, "f16c": 36, "f16x": 36}
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes per node update of the bulk kernel from ncu, per (precision, staged):
 # dram__bytes_read.sum + dram__bytes_write.sum of both launches of one staged step of the
@@ -515,7 +515,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["vortexlab", "reference"], default="vortexlab")
-    ap.add_argument("--precision", choices=["f64", "f32", "f16s", "f16c"], default="f64")
+    ap.add_argument("--precision", choices=["f64", "f32", "f16s", "f16c", "f16x"], default="f64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-parity", action="store_true")

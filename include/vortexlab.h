@@ -46,8 +46,11 @@ extern "C" {
 enum { VL_BGK = 0, VL_TRT = 1 };                              /* src/lattice.rs:28-35 */
 /* population storage: FP64; FP32; IEEE FP16 of f_i - w_i; 16-bit f_i - w_i with a sign, a 3-bit
  * exponent and a 12-bit mantissa (2^(e-9) (1 + m/4096), evenly spaced by 2^-20 below 2^-8,
- * saturating at 0.49994). The narrow formats collide in FP32 and sum forces in FP64. */
-enum { VL_F64 = 0, VL_F32 = 1, VL_F16S = 2, VL_F16C = 3 };
+ * saturating at 0.49994); 16-bit fixed point of f_i - w_i (steps 2^-19 for the rest population
+ * and the diagonals, 2^-18 for the axis directions, saturating at +-0.0625 / +-0.125). The
+ * narrow formats collide in FP32 and sum forces in FP64; the saturating ones report a density
+ * leaving 1 +- 1/2 as divergence. */
+enum { VL_F64 = 0, VL_F32 = 1, VL_F16S = 2, VL_F16C = 3, VL_F16X = 4 };
 enum { VL_VEL_NONE = 0, VL_VEL_CONST = 1, VL_VEL_PARABOLIC = 2, VL_VEL_ROTATION = 3 };
 enum { VL_CORNER_SHARP = 0, VL_CORNER_CHAMFERED = 1, VL_CORNER_ROUNDED = 2,
        VL_CORNER_RECESSED = 3, VL_CORNER_DOUBLE_RECESSED = 4 }; /* src/geometry.rs:188-201 */

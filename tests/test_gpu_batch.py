@@ -13,7 +13,7 @@ def _cases(V):
     return cases
 
 
-@pytest.mark.parametrize("prec", ["f64", "f32", "f16s"])
+@pytest.mark.parametrize("prec", ["f64", "f32", "f16s", "f16x"])
 def test_batched_tunnels_match_single_runs(gpu, prec):
     """Every tile shape and schedule, and for the narrow formats both bulk forms (two cells per
     thread, one): the batched tunnel's populations and force history are bit-identical to the

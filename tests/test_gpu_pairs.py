@@ -35,7 +35,7 @@ def _domains():
 
 
 def _aligned(d, prec):
-    elem = {"f64": 8, "f32": 4, "f16s": 2, "f16c": 2}[prec]
+    elem = {"f64": 8, "f32": 4, "f16s": 2, "f16c": 2, "f16x": 2}[prec]
     return d["nx"] * elem % 16 == 0
 
 
@@ -65,7 +65,7 @@ def _run(d, prec, schedule, cells, steps, copies=True, prefetch=0):
     return sim.populations(), sim.history()
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c"])
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c", "f16x"])
 @pytest.mark.parametrize("name", list(_domains().keys()))
 def test_two_cell_kernel_matches_one_cell_kernel(gpu, prec, name):
     d = _domains()[name]

@@ -1,4 +1,4 @@
-"""Reduced-precision storage (FP32; FP16 of f_i - w_i) with FP32 collision and FP64 force,
+"""Reduced-precision storage (FP32; 16-bit forms of f_i - w_i) with FP32 collision and FP64 force,
 compared with the FP64 path (which is bit-identical to the reference's CPU solver)."""
 import numpy as np
 import pytest
@@ -23,7 +23,18 @@ def c16_stored(v32, w32):
     return (x + w32.astype(np.float64)).astype(np.float32)
 
 
-@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c"])
+def q16_stored(v32, w32, up):
+    """The value the 16-bit fixed-point format stores for FP32 populations v32 of weight w32 with
+    scale `up` (2^18 for the axis directions, 2^19 otherwise), restated on the host: (v - w) up
+    rounded once to FP32 (the scale is a power of two, so that is the FP32 difference scaled),
+    rounded to the nearest integer (ties to even) and clamped to int16, then decoded and w added
+    back in one FP32 rounding."""
+    y = (v32 - w32).astype(np.float32) * np.float32(up)
+    q = np.clip(np.rint(y), -32768, 32767).astype(np.float32)
+    return (w32 + q * np.float32(1.0 / up)).astype(np.float32)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f16s", "f16c", "f16x"])
 def test_storage_round_trip(gpu, prec):
     """Sim::init writes equilibria; the download returns them rounded to the storage format."""
     V = gpu
@@ -41,6 +52,10 @@ def test_storage_round_trip(gpu, prec):
     elif prec == "f16c":
         w32 = np.broadcast_to(w[:, None, None].astype(np.float32), fe.shape)
         expect = c16_stored(fe.astype(np.float32), w32).astype(np.float64)
+    elif prec == "f16x":
+        w32 = np.broadcast_to(w[:, None, None].astype(np.float32), fe.shape)
+        up = np.array([2.0 ** 19] + [2.0 ** 18] * 4 + [2.0 ** 19] * 4)[:, None, None]
+        expect = np.stack([q16_stored(fe[i].astype(np.float32), w32[i], up[i, 0, 0]) for i in range(9)]).astype(np.float64)
     else:
         expect = (w[:, None, None].astype(np.float32)
                   + (fe.astype(np.float32) - w[:, None, None].astype(np.float32)).astype(np.float16).astype(np.float32)
@@ -61,7 +76,7 @@ def test_f32_schafer_turek_2d2_matches_f64(gpu):
         assert abs(vb - va) <= tol * abs(va), (k, va, vb)
 
 
-@pytest.mark.parametrize("prec,tol", [("f32", 1e-6), ("f16s", 5e-4), ("f16c", 5e-4)])
+@pytest.mark.parametrize("prec,tol", [("f32", 1e-6), ("f16s", 5e-4), ("f16c", 5e-4), ("f16x", 5e-4)])
 def test_decaying_swirl_matches_f64(gpu, prec, tol):
     """Periodic box, TRT, 400 steps of a decaying swirl: velocity and density fields against FP64."""
     d = S.periodic_box(48, 36, 0.62, ("trt", 3.0 / 16.0))

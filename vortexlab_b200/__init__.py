@@ -31,7 +31,7 @@ __all__ = [
 ]
 
 FLUID = 0
-PRECISIONS = {"f64": 0, "f32": 1, "f16s": 2, "f16c": 3}
+PRECISIONS = {"f64": 0, "f32": 1, "f16s": 2, "f16c": 3, "f16x": 4}
 CS2 = 1.0 / 3.0
 
 

@@ -548,6 +548,7 @@ vl_sim* make_sim(vl::CompiledDomain&& dom, int precision) {
     case VL_F32: s->L = &vl::launchers_f32(); break;
     case VL_F16S: s->L = &vl::launchers_f16s(); break;
     case VL_F16C: s->L = &vl::launchers_f16c(); break;
+    case VL_F16X: s->L = &vl::launchers_f16x(); break;
     default: fail(VL_EINVAL, "unknown precision"); return nullptr;
   }
   s->dom = std::move(dom);

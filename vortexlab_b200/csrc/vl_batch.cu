@@ -369,6 +369,7 @@ vl_batch* vl_batch_new(int precision) {
     case VL_F32: L = &vl::launchers_f32(); break;
     case VL_F16S: L = &vl::launchers_f16s(); break;
     case VL_F16C: L = &vl::launchers_f16c(); break;
+    case VL_F16X: L = &vl::launchers_f16x(); break;
     default: fail(VL_EINVAL, "unknown precision"); return nullptr;
   }
   auto b = new vl_batch();

@@ -49,5 +49,6 @@ const Launchers& launchers_f64();
 const Launchers& launchers_f32();
 const Launchers& launchers_f16s();
 const Launchers& launchers_f16c();
+const Launchers& launchers_f16x();
 
 }  // namespace vl

@@ -68,6 +68,23 @@ struct Codec16<c16> {
   }
 };
 
+// The 16-bit fixed-point format (q16, vl_device.cuh): the two codes of a word convert to FP32
+// exactly and one packed fused multiply-add scales them and adds w_i; encoding is the packed fused
+// multiply-add that scales and subtracts w_i, then a saturating conversion of each to int16.
+template <>
+struct Codec16<q16> {
+  static __device__ __forceinline__ float2 dec(int i, unsigned w) {
+    const float2 x = make_float2((float)(int)(short)(w & 0xffffu), (float)((int)w >> 16));
+    const float d = q16f::down(i), wi = wgt<float>(i);
+    return __ffma2_rn(x, make_float2(d, d), make_float2(wi, wi));
+  }
+  static __device__ __forceinline__ unsigned enc(int i, float2 f) {
+    const float u = q16f::up(i), sw = -wgt<float>(i) * u;
+    const float2 y = __ffma2_rn(f, make_float2(u, u), make_float2(sw, sw));
+    return ((unsigned)q16f::code(y.x) & 0xffffu) | ((unsigned)q16f::code(y.y) << 16);
+  }
+};
+
 // ------------------------------------------------------------------ vector access per format
 // `Word` holds a thread's V stored values; dec / left / right give the V / 2 FP32 pairs of the
 // aligned group, of the group shifted one cell left (x0 - 1 ..) and one cell right (x0 + 1 ..);

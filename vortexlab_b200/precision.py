@@ -22,7 +22,7 @@ import numpy as np
 from . import cylinder, section, signal
 from .tunnel import Tunnel
 
-PRECISIONS = ("f64", "f32", "f16s", "f16c")
+PRECISIONS = ("f64", "f32", "f16s", "f16c", "f16x")
 
 
 def cylinder_2d2(n=80, units=100.0, window=20.0, precisions=PRECISIONS):
@@ -66,12 +66,16 @@ def relative_errors(table, ref="f64", keys=None):
 if __name__ == "__main__":
     import json
     import sys
+    # python -m vortexlab_b200.precision [both|cylinder|square] [f64,f32,...]   (f64 always included)
     which = sys.argv[1] if len(sys.argv) > 1 else "both"
+    precs = PRECISIONS
+    if len(sys.argv) > 2:
+        precs = tuple(["f64"] + [p for p in sys.argv[2].split(",") if p != "f64"])
     res = {}
     if which in ("both", "cylinder"):
-        t = cylinder_2d2()
+        t = cylinder_2d2(precisions=precs)
         res["cylinder_2d2_n80"] = {"values": t, "rel_error_vs_f64": relative_errors(t)}
     if which in ("both", "square"):
-        t = square_tunnel()
+        t = square_tunnel(precisions=precs)
         res["square_d60_re150"] = {"values": t, "rel_error_vs_f64": relative_errors(t)}
     print(json.dumps(res, indent=1, default=float))
