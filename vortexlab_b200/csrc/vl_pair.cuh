@@ -97,6 +97,13 @@ struct GroupIO<float, 2> {
   using Word = float2;
   template <bool SM>
   static __device__ __forceinline__ Word ld(const float* p) {
+#ifdef VL_LD_L2_256B
+    if (!SM) {
+      float2 w;
+      asm("ld.global.nc.L2::256B.v2.f32 {%0, %1}, [%2];" : "=f"(w.x), "=f"(w.y) : "l"(p));
+      return w;
+    }
+#endif
     return SM ? *reinterpret_cast<const float2*>(p) : __ldg(reinterpret_cast<const float2*>(p));
   }
   static __device__ __forceinline__ void st(float* p, Word w) { *reinterpret_cast<float2*>(p) = w; }
