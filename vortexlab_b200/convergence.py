@@ -249,11 +249,13 @@ if __name__ == "__main__":
     import json
     import sys
     what = sys.argv[1] if len(sys.argv) > 1 else "study"
+    # python -m vortexlab_b200.convergence throughput [max_steps schedule precision cells prefetch count]
     if what == "throughput":
         print(json.dumps(throughput(max_steps=int(sys.argv[2]) if len(sys.argv) > 2 else 0,
                                     schedule=sys.argv[3] if len(sys.argv) > 3 else "concurrent",
                                     precision=sys.argv[4] if len(sys.argv) > 4 else "f32",
                                     cells=int(sys.argv[5]) if len(sys.argv) > 5 else 2,
-                                    prefetch=int(sys.argv[6]) if len(sys.argv) > 6 else -1), default=float))
+                                    prefetch=int(sys.argv[6]) if len(sys.argv) > 6 else -1,
+                                    count=int(sys.argv[7]) if len(sys.argv) > 7 else 256), default=float))
     else:
         print(json.dumps(study(subset=int(sys.argv[2]) if len(sys.argv) > 2 else 32), default=float, indent=1))
