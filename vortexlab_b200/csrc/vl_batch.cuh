@@ -105,17 +105,28 @@ __device__ __forceinline__ void packed_seg(const int4& td, int nx, int seg, int 
 // `width`: the tile's width in cells, or in the packed layout the segment's.
 template <class S>
 __device__ __forceinline__ void batch_prefetch(const BatchParams& p, const S* A, int k, int width) {
-  const int rows = p.packed ? kBlock / 32 : p.ty;
+  // packed layout: the tile's 8 segments are one stretch of the tunnel's rows laid end to end, so
+  // they cover contiguous spans of at most three rows where a row holds 4 or more segments (the
+  // spans of any further rows are not asked for: this is a hint)
+  const int rows = p.packed ? 3 : p.ty;
   if (k >= p.ntiles || (int)threadIdx.x >= 9 * rows) return;
   const int4 td = __ldg(p.tiles + k);
   const BatchTunnel& T = p.tun[td.x];
   const int i = (int)threadIdx.x % 9, j = (int)threadIdx.x / 9;
-  int y = td.y + j, x0 = td.z;
-  if (p.packed) packed_seg(td, T.nx, width, j, y, x0);
+  int y = td.y + j, x0 = td.z, end = x0 + width;
+  if (p.packed) {
+    int y0, xf, yl, xl;
+    packed_seg(td, T.nx, width, 0, y0, xf);
+    packed_seg(td, T.nx, width, kBlock / 32 - 1, yl, xl);
+    y = y0 + j;
+    if (y > yl) return;
+    x0 = j == 0 ? xf : 0;
+    end = y == yl ? xl + width : T.nx;
+  }
   if (y >= T.ny) return;
   const int ym = y == 0 ? T.ny - 1 : y - 1, yp = y == T.ny - 1 ? 0 : y + 1;
   const int r = (i == 2 || i == 5 || i == 6) ? ym : ((i == 4 || i == 7 || i == 8) ? yp : y);
-  const int end = min(x0 + width, T.nx);
+  end = min(end, T.nx);
   if (end <= x0) return;
   prefetch_l2(A + T.pop_off + (size_t)i * T.ns + (size_t)r * T.nx + x0, (size_t)(end - x0) * sizeof(S));
 }
