@@ -3,9 +3,9 @@ used to exercise it.
 
 ``Batch`` packs channels of uneven sizes, shapes and Reynolds numbers into one device arena and
 advances them together, each for its own number of steps; every tunnel follows Channel::step
-(src/cases/channel.rs:118-130) exactly, so in FP64 a tunnel in a batch is bit-identical to the same
-tunnel run alone (in FP32 / FP16 it agrees to rounding: those kernels are compiled with multiply-add
-contraction, which the compiler may place differently in the batched and the single kernels).
+(src/cases/channel.rs:118-130) exactly, so a tunnel in a batch is bit-identical to the same tunnel
+run alone (FP64: the reference's operation order; the narrow formats: the explicitly rounded FP32
+collision that every narrow kernel shares).
 ``seeded_tunnels`` draws the bodies and flow parameters of the batched workload.
 """
 from __future__ import annotations
