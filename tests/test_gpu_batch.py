@@ -219,6 +219,8 @@ def test_held_tunnel_started_later_runs_as_from_step_zero(gpu):
     b.run_async(37)
     b.wait()
     assert b.status(1)[0] == 0
+    with pytest.raises(V.VortexError):
+        b.hold(2)                       # only before the batch's first step
     b.run_async(10)                     # global steps 37..47 in flight
     assert b.start(1) == 47             # its step 0 follows them (an odd global step: the other buffer)
     b.set_steps(1, 50)                  # 50 of its own steps
